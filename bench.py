@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark of the direct-summation gravity path on B200.
+
+Metric: G pair-interactions/s of the split-FP32 kernel (pairs = sum over sets
+of N_s^2, self pair included), with the plain FP64 GPU kernel, the accuracy of
+split-FP32 against it, and the reference's CPU path (C restatement of
+cpu_grav.f) on a bounded sample reported beside it.
+
+One step = one gravity call over the whole workload with inputs resident in
+HBM (``value``); ``e2e`` repeats it through the reference-facing Fortran
+C-ABI (firsthalf_grav_forces_/lasthalf_grav_forces_) from host arrays, copies
+included.  Default workload: config3, the N=1,048,576 red-giant model.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload config1..config5]
+
+Multi-GPU (torchrun): every rank evaluates its own independent copy of the
+workload (a different seed: independent stellar models, no data-path
+collective), ``value`` = all ranks' pairs / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "G pair-interactions/s: split-FP32 vs plain FP64 GPU at <=1e-6 rel accel error"
+UNIT = "G pair-interactions/s"
+FLOPS_PER_PAIR = 20  # far-field acc + pot convention (FMA = 2, rsqrt = 1)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="config3")
+    p.add_argument("--precision", default="f32split", choices=["f32split", "fp64"])
+    p.add_argument("--nkernel", type=int, default=0)
+    p.add_argument("--cpu-seconds", type=float, default=15.0,
+                   help="target length of the CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(ws, target_s: float, rank_seed_rows: int = 0):
+    """The reference's CPU path (oracle: C restatement of cpu_grav.f, the
+    j >= i triangle with Newton's third law, all host cores) on a bounded
+    sample of rows of the same workload; credited ordered pairs = 2 x triangle
+    evaluations - self pairs."""
+    import oracle
+    threads = oracle.max_threads()
+    results = []
+    total_pairs = 0
+    total_t = 0.0
+    for s in range(ws.nsets):
+        if total_t >= target_s:
+            break
+        a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
+        n = b - a
+        x, y, z, m, r2 = (arr[a:b] for arr in (ws.x, ws.y, ws.z, ws.m, ws.range2))
+        # calibrate on a short slice in the middle of the triangle
+        lo = n // 3
+        rows = max(threads, min(n - lo, 2 * threads))
+        t0 = time.perf_counter()
+        oracle.triangle(x, y, z, m, r2, 0, lo, lo + rows, threads)
+        dt = time.perf_counter() - t0
+        evals = sum(n - i for i in range(lo, lo + rows))
+        rate = evals / max(dt, 1e-9)
+        want = max(0.0, target_s - total_t) * rate
+        hi = lo
+        acc = 0
+        while hi < n and acc < want:
+            acc += n - hi
+            hi += 1
+        hi = max(hi, lo + 1)
+        t0 = time.perf_counter()
+        oracle.triangle(x, y, z, m, r2, 0, lo, hi, threads)
+        dt = time.perf_counter() - t0
+        evals = sum(n - i for i in range(lo, hi))
+        credited = 2 * evals - (hi - lo)
+        total_pairs += credited
+        total_t += dt
+        results.append({"set": s, "rows": [lo, hi], "seconds": dt})
+    value = total_pairs / total_t / 1e9
+    sample = ("triangle rows " + ", ".join(f"set{r['set']}[{r['rows'][0]}:{r['rows'][1]}]"
+                                           for r in results)
+              + f" of {ws.name}; {total_pairs:.3e} credited ordered pairs in {total_t:.1f} s")
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+
+def load_workload(name: str, rank: int):
+    from starsmasher_b200 import inputs
+    seed = {"config1": 1, "config2": 2, "config3": 3, "config4": 4, "config5": 5}[name] + 100 * rank
+    return inputs.cached(name, seed=seed)
+
+
+def run_reference_arm(args, world, rank):
+    """--impl reference: the reference's CPU gravity path (the Fortran does
+    not compile here -- no Fortran compiler -- so its C restatement in
+    oracle/ is timed) on all host cores, K bounded samples of the workload."""
+    if rank != 0:
+        return
+    ws = load_workload(args.workload, 0)
+    for _ in range(args.warmup):
+        cpu_baseline(ws, 0.5)
+    vals = []
+    last = None
+    t_all = time.perf_counter()
+    per_step = max(2.0, args.cpu_seconds / max(1, args.steps))
+    for _ in range(args.steps):
+        last = cpu_baseline(ws, per_step)
+        vals.append(last["value"])
+    elapsed = time.perf_counter() - t_all
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": ws.name, "n": ws.n, "nsets": ws.nsets, "pairs_per_step": ws.pairs,
+                   "nkernel": 0, "algorithm": "cpu_grav.f triangle (C restatement), sampled rows"},
+        "cpu_baseline": dict(last, value=value),
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from starsmasher_b200 import Context, api, launch_count
+
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+
+    ws = load_workload(args.workload, rank)
+    n = ws.n
+    pairs = ws.pairs
+    batched = ws.nsets > 1
+
+    stream = torch.cuda.current_stream()
+    ctx = Context(device)
+    ctx.set_stream(stream.cuda_stream)
+
+    dt = torch.float64
+    X = [torch.as_tensor(a).to(device=f"cuda:{device}", dtype=dt)
+         for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
+    outs = [torch.empty(n, dtype=dt, device=f"cuda:{device}") for _ in range(4)]
+    W = torch.empty(ws.nsets, dtype=dt, device=f"cuda:{device}")
+
+    def step(precision):
+        if batched:
+            ctx.batch_forces_device(ws.offsets, *X, *outs, W=W, nkernel=args.nkernel,
+                                    precision=precision)
+        else:
+            ctx.forces_device(n, *X, *outs, W=W, nkernel=args.nkernel, precision=precision)
+
+    # L2 flush buffer (> 126 MB L2), written between timed steps
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")
+
+    for _ in range(max(3, args.warmup)):
+        step(args.precision)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ------------------------------------------------------- timed region
+    ctx.profile_enable(True)
+    ctx.profile_read()
+    clocks = Clocks(device)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = launch_count()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(args.precision)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier()
+    launches = launch_count() - l0
+    clk = clocks.stop()
+    kern_ms, kern_n = ctx.profile_read()
+    ctx.profile_enable(False)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = pairs * world * args.steps / (total_ms * 1e-3) / 1e9
+    res_f32 = [o.cpu().numpy() for o in outs]
+
+    # --------------------------------------------- FP64 kernel and accuracy
+    fp64 = None
+    acc = None
+    if not args.no_fp64:
+        step("fp64")
+        torch.cuda.synchronize()
+        reps = 2
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            step("fp64")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1) / reps
+        v64 = pairs / (ms64 * 1e-3) / 1e9
+        res64 = [o.cpu().numpy() for o in outs]
+        num = np.sqrt(sum((a - b) ** 2 for a, b in zip(res_f32[:3], res64[:3])))
+        amag = np.sqrt(sum(b ** 2 for b in res64[:3]))
+        e = num / amag
+        ill = amag < 1e-3 * np.median(amag)
+        ep = np.abs(res_f32[3] - res64[3]) / np.abs(res64[3])
+        acc = {"reference": "plain FP64 GPU kernel, all rows",
+               "acc_rel_max": float(e[~ill].max()), "acc_rel_rms": float(np.sqrt(np.mean(e[~ill] ** 2))),
+               "acc_rel_max_illconditioned": float(e[ill].max()) if ill.any() else None,
+               "n_illconditioned": int(ill.sum()),
+               "pot_rel_max": float(ep.max()), "pot_rel_rms": float(np.sqrt(np.mean(ep ** 2)))}
+        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64, "speedup_f32split_vs_fp64": value / world / v64}
+
+    # ------------------------------------------------------------ roofline
+    peak = ctx.fp32_peak_probe(200000)
+    kernel_ms = kern_ms / max(1, kern_n)
+    achieved = pairs * FLOPS_PER_PAIR / (kernel_ms * 1e-3) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", f"traffic_{args.precision}.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tb = json.load(f).get("dram_bytes_per_pair")
+        if tb:
+            traffic = tb * pairs
+    roofline = {"bound": "fp32-fma", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel_ms_per_launch": kernel_ms, "flops_per_pair": FLOPS_PER_PAIR,
+                "peak_source": "measured in-run: packed-FFMA throughput probe on this GPU "
+                               "(MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
+                "time_share_kernel": kernel_ms / ms_per_step if ms_per_step else None}
+
+    # ----------------------------------------------------------------- e2e
+    e2e = None
+    if not args.no_e2e:
+        if batched:
+            def e2e_step():
+                ctx.batch_forces(ws.offsets, ws.x, ws.y, ws.z, ws.m, ws.range2, args.nkernel,
+                                 args.precision)
+            how = "sphgrav_batch_forces (host arrays)"
+        else:
+            api.gpu_init_dev(device, 0.3)
+            api.set_legacy_precision(args.precision)
+            gx, gy, gz, gp = (np.zeros(n) for _ in range(4))
+
+            def e2e_step():
+                api.firsthalf_grav_forces(n, 1, n, ws.x, ws.y, ws.z, ws.m, ws.range2, 1,
+                                          args.nkernel)
+                api.lasthalf_grav_forces(n, gx, gy, gz, gp)
+            how = "firsthalf_grav_forces_/lasthalf_grav_forces_ (Fortran C-ABI, host arrays)"
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        t_e2e = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{device}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e = {"value": pairs * world * args.steps / t_e2e / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 5 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n,
+               "ms_per_step": t_e2e / args.steps * 1e3, "path": how}
+
+    # -------------------------------------------------------- CPU baseline
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(ws, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "f32split" else "f64",
+            "data": "synthetic: seeded polytropic star models (no public dataset), one independent model per rank",
+            "config": {"workload": ws.name, "n": n, "nsets": ws.nsets, "pairs_per_step": pairs,
+                       "precision": args.precision, "nkernel": args.nkernel,
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"replicas x{world} (independent models per GPU)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "fp64": fp64, "accuracy_vs_fp64": acc,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * sphgrav_b200.h -- direct-summation SPH self-gravity for NVIDIA B200 (sm_100a).
+ *
+ * Drop-in replacement for StarSmasher's SPHgrav_lib2 (libSPHgrav.a).  All
+ * citations are paths inside the reference project.
+ *
+ * Physics (both precisions): every listed row i receives
+ *     a_i   = sum_j  m_j f(r_ij; H_i, H_j) (x_j - x_i)
+ *     phi_i = sum_j  m_j g(r_ij; H_i, H_j)
+ * with H = sqrt(|range2|) = 2 hp, Newtonian when r^2 >= max(H_i^2, H_j^2) and
+ * the symmetrised softening of kernel `nkernel` otherwise (0 cubic spline,
+ * 1 Wendland C6, 2 Wendland C4), exactly as the reference's CPU path
+ * parallel_bleeding_edge/src/cpu_grav.f:1-381 evaluates it (G = 1).
+ * Point masses carry range2 < 0 (grav.f:15-18): no self-potential.
+ *
+ * Precisions:
+ *   SPHGRAV_FP64       plain FP64 kernel; matches the CPU path to ~1e-12.
+ *   SPHGRAV_F32SPLIT   positions as FP32 hi+lo pairs, pair sums in FP32 with one
+ *                      Newton step per rsqrt and compensated (Kahan/TwoSum)
+ *                      partial sums; FP64 for the split, the cross-block
+ *                      partial sums, the near-field (r < max H) pairs and the
+ *                      potential-energy diagnostic.  Max relative error of the
+ *                      acceleration is ~1e-6 or better for well-conditioned
+ *                      particles.
+ *
+ * Threading: a context is used by one host thread at a time.  Calls enqueue
+ * work on the context's stream; functions that return results to host
+ * memory synchronise that stream.
+ */
+#ifndef SPHGRAV_B200_H
+#define SPHGRAV_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    SPHGRAV_OK = 0,
+    SPHGRAV_ERR_INVALID_ARGUMENT = 1,  /* bad size, pointer, nkernel, precision */
+    SPHGRAV_ERR_INVALID_INPUT = 2,     /* mass <= 0, range2 == 0, non-finite value */
+    SPHGRAV_ERR_CUDA = 3,              /* CUDA runtime error (see sphgrav_last_error_message) */
+    SPHGRAV_ERR_NO_DEVICE = 4,
+    SPHGRAV_ERR_OUT_OF_MEMORY = 5,
+    SPHGRAV_ERR_PROTOCOL = 6,          /* lasthalf without firsthalf, and similar */
+    SPHGRAV_ERR_DEVICE_TIMEOUT = 7,    /* a bounded device-side wait gave up */
+    SPHGRAV_ERR_TOO_LARGE = 8          /* size beyond a documented limit */
+};
+
+enum { SPHGRAV_FP64 = 0, SPHGRAV_F32SPLIT = 1 };
+
+typedef struct sphgrav_ctx sphgrav_ctx;
+typedef struct sphgrav_graph sphgrav_graph;
+
+/* ------------------------------------------------- legacy Fortran ABI ---
+ * Same symbols, argument lists and call protocol as the reference library;
+ * Fortran passes every argument by reference.  On error these log to stderr
+ * and abort, as the reference's assert/exit does (cutil.h:19-27).
+ * Precision: SPHGRAV_F32SPLIT unless the environment variable
+ * SPHGRAV_PRECISION=fp64 is set (or sphgrav_legacy_set_precision is called).
+ */
+
+/* Replaces firsthalf_grav_forces_ (grav_force_direct.cu:650-656), called from
+ * grav.f:25-26, eatem.f:161 and main.f:362-374.  n particles, rows
+ * [n_lower, n_lower + my_length) (1-based n_lower) are computed; q is ignored
+ * like the reference's (:653-655).  Copies the inputs, enqueues the
+ * computation and returns without waiting for it. */
+void firsthalf_grav_forces_(int *n, int *n_lower, int *my_length,
+                            double *px, double *py, double *pz,
+                            double *mass, double *range2, int *q, int *nkernel);
+
+/* Replaces lasthalf_grav_forces_ (grav_force_direct.cu:658-664), called from
+ * balAV3.f:418 and eatem.f:163.  Waits for the result of the last
+ * firsthalf_grav_forces_ and writes ax, ay, az, pot at the rows that call
+ * listed (arrays of length n).  myrank is never read: the Fortran callers pass
+ * only five arguments. */
+void lasthalf_grav_forces_(int *n, double *ax, double *ay, double *az,
+                           double *pot, int *myrank);
+
+/* Replaces gpu_init_dev_ (grav_force_direct.cu:672-675), called from
+ * main.f:265-275.  Selects CUDA device *myrank; theta is ignored (it is the
+ * opening angle of the tree plugin). */
+void gpu_init_dev_(int *myrank, double *theta);
+
+/* Precision used by the three legacy entry points (SPHGRAV_FP64 or
+ * SPHGRAV_F32SPLIT).  No reference counterpart (the reference is FP32 only,
+ * grav_force_direct.cu:55-396). */
+int sphgrav_legacy_set_precision(int precision);
+
+/* ------------------------------------------------------- context API ---
+ * Status-returning twins of the legacy entry points, plus the batch API.
+ * No reference counterparts unless stated. */
+int sphgrav_create(sphgrav_ctx **ctx, int device);
+int sphgrav_destroy(sphgrav_ctx *ctx);
+/* Use an existing cudaStream_t (passed as void*) instead of the context's
+ * own stream; NULL restores the context's stream. */
+int sphgrav_set_stream(sphgrav_ctx *ctx, void *stream);
+/* Wait for all work queued on the context and report a device-side error
+ * (invalid input found on the device, timeout) recorded since the last call. */
+int sphgrav_sync(sphgrav_ctx *ctx);
+
+/* Status-returning twin of firsthalf_grav_forces_: host arrays of length n,
+ * rows [i_begin, i_begin + ni) with 0-based i_begin. */
+int sphgrav_firsthalf(sphgrav_ctx *ctx, int n, int i_begin, int ni,
+                      const double *x, const double *y, const double *z,
+                      const double *mass, const double *range2,
+                      int nkernel, int precision);
+/* Status-returning twin of lasthalf_grav_forces_: writes rows
+ * [i_begin, i_begin + ni) of the host arrays (length n). */
+int sphgrav_lasthalf(sphgrav_ctx *ctx, double *ax, double *ay, double *az,
+                     double *pot);
+
+/* Host-side restatement of the Fortran caller: gravforce (grav.f:12-26)
+ * builds range2 = 4 hp^2, negated where u == 0, and calls firsthalf for rows
+ * [ngrav_lower, ngrav_upper] (1-based, inclusive, as main.f:283-295 sets
+ * them); lasthalf (balAV3.f:418) then fills gx, gy, gz, grpot at those rows.
+ * Host arrays of length ntot.  Blocking. */
+int sphgrav_gravforce(sphgrav_ctx *ctx, int ntot, int ngrav_lower, int ngrav_upper,
+                      const double *x, const double *y, const double *z,
+                      const double *am, const double *hp, const double *u,
+                      int nkernel, int precision,
+                      double *gx, double *gy, double *gz, double *grpot);
+
+/* One particle set, all pointers DEVICE pointers of length n; rows
+ * [i_begin, i_begin + ni) of the outputs are written.  Asynchronous on the
+ * context's stream; W (device pointer to one double, may be NULL) receives
+ * 0.5 * sum_rows m_i phi_i (output.f:232-252 computes it on the host). */
+int sphgrav_forces_device(sphgrav_ctx *ctx, int n, int i_begin, int ni,
+                          const double *x, const double *y, const double *z,
+                          const double *mass, const double *range2,
+                          int nkernel, int precision,
+                          double *ax, double *ay, double *az, double *pot,
+                          double *W);
+
+/* Batch of independent particle sets in one persistent launch.  Set s holds
+ * particles [offsets[s], offsets[s+1]) of the concatenated arrays; offsets is
+ * a HOST array of nsets+1 ints.  Data pointers are DEVICE pointers.  All rows
+ * of every set are computed; W_per_set (device, nsets doubles, may be NULL)
+ * receives each set's 0.5 * sum m_i phi_i.  Asynchronous. */
+int sphgrav_batch_forces_device(sphgrav_ctx *ctx, int nsets, const int *offsets,
+                                const double *x, const double *y, const double *z,
+                                const double *mass, const double *range2,
+                                int nkernel, int precision,
+                                double *ax, double *ay, double *az, double *pot,
+                                double *W_per_set);
+
+/* Same with HOST data pointers; copies in, computes, copies out, returns
+ * when the results are in host memory. */
+int sphgrav_batch_forces(sphgrav_ctx *ctx, int nsets, const int *offsets,
+                         const double *x, const double *y, const double *z,
+                         const double *mass, const double *range2,
+                         int nkernel, int precision,
+                         double *ax, double *ay, double *az, double *pot,
+                         double *W_per_set);
+
+/* ---------------------------------------------- device-resident sweeps --- */
+/* Add a seeded Gaussian displacement of standard deviation sigma to the n
+ * device positions.  The draw for call c of particle p depends only on
+ * (seed, c, p); c is a device-side counter that this kernel increments, so
+ * repeated replays of a captured graph draw fresh kicks. */
+int sphgrav_kick_positions_device(sphgrav_ctx *ctx, int n, double *x, double *y,
+                                  double *z, double sigma, unsigned long long seed);
+/* Reset the kick call counter to c (device-side, asynchronous). */
+int sphgrav_kick_reset(sphgrav_ctx *ctx, unsigned long long c);
+
+/* Capture the context's work between begin and end into a CUDA graph.
+ * Inside the capture only *_device entry points may be called, and each of
+ * them must have been called once before with the same sizes, so that every
+ * buffer already exists. */
+int sphgrav_capture_begin(sphgrav_ctx *ctx);
+int sphgrav_capture_end(sphgrav_ctx *ctx, sphgrav_graph **graph);
+int sphgrav_graph_launch(sphgrav_graph *graph, int repeats);
+int sphgrav_graph_destroy(sphgrav_graph *graph);
+
+/* ------------------------------------------------------------ tuning --- */
+/* Time the kernel variants on the sets described by (nsets, offsets) with the
+ * given device data and keep the fastest per (precision, N bucket).  Later
+ * calls in that bucket use it. */
+int sphgrav_autotune(sphgrav_ctx *ctx, int nsets, const int *offsets,
+                     const double *x, const double *y, const double *z,
+                     const double *mass, const double *range2,
+                     int nkernel, int precision);
+/* Persist / restore the tuning table (a small JSON file). */
+int sphgrav_tuning_save(sphgrav_ctx *ctx, const char *path);
+int sphgrav_tuning_load(sphgrav_ctx *ctx, const char *path);
+/* Force a kernel variant by index (-1 = automatic) for a precision. */
+int sphgrav_force_variant(sphgrav_ctx *ctx, int precision, int variant);
+/* Number of kernel variants and a printable name of each. */
+int sphgrav_variant_count(int precision);
+const char *sphgrav_variant_name(int precision, int variant);
+
+/* ------------------------------------------------------- diagnostics --- */
+const char *sphgrav_status_string(int status);
+/* Last error message recorded on this thread (CUDA error text and context). */
+const char *sphgrav_last_error_message(void);
+/* Kernels launched by this library since the process started. */
+unsigned long long sphgrav_launch_count(void);
+/* Work items and j-chunks of the last computation (for tests and tuning). */
+int sphgrav_last_plan_info(sphgrav_ctx *ctx, int *nitems, int *nchunks_max,
+                           int *variant);
+/* Kernel timing: while enabled, CUDA events are recorded on the context's
+ * stream around every pair-sum kernel launch (not inside graph captures);
+ * sphgrav_profile_read returns the summed kernel milliseconds and launch
+ * count since the previous read (it synchronises the stream). */
+int sphgrav_profile_enable(sphgrav_ctx *ctx, int on);
+int sphgrav_profile_read(sphgrav_ctx *ctx, double *kernel_ms, int *launches);
+/* FP32 FMA throughput probe: runs a packed-FMA loop for about `iters`
+ * iterations per thread on the context's device and returns the measured
+ * TFLOP/s (2 flops per FMA) in *tflops. */
+int sphgrav_fp32_peak_probe(sphgrav_ctx *ctx, int iters, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHGRAV_B200_H */

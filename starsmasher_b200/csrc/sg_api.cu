@@ -1,0 +1,1176 @@
+// sg_api.cu -- host runtime of the B200 gravity library: contexts, device
+// buffers, work plans, the per-call pipeline, the legacy Fortran ABI, the
+// batch and capture entry points and the autotuner.
+//
+// Reference host code replaced (parallel_bleeding_edge/src/SPHgrav_lib2/):
+//   grav_force_direct.cu:504-646  SPHgrav_direct / SPHgrav:: marshalling.  The
+//     reference re-allocates its buffers and converts positions to float on
+//     the host every call; here buffers grow once and stay on the device, the
+//     conversion, sort and tiling run as kernels, and host<->device copies
+//     are one contiguous transfer each way.
+//   grav_force_direct.cu:648-677  the C-ABI (same symbols below).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#include "sg_launch.h"
+#include "../../include/sphgrav_b200.h"
+
+namespace sg {
+int f64_variant_count();
+const VariantInfo &f64_variant_info(int v);
+const void *f64_kernel(int v);
+cudaError_t launch_f64(int v, int grid, const ComputeArgs &a, cudaStream_t st);
+int f32_variant_count();
+const VariantInfo &f32_variant_info(int v);
+const void *f32_kernel(int v);
+cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st);
+
+int variant_count(int precision) { return precision == 0 ? f64_variant_count() : f32_variant_count(); }
+const VariantInfo &variant_info(int precision, int v)
+{
+    return precision == 0 ? f64_variant_info(v) : f32_variant_info(v);
+}
+int variant_occupancy(int precision, int v)
+{
+    static std::map<std::pair<int, int>, int> cache;
+    auto key = std::make_pair(precision, v);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int nb = 0;
+    const void *k = precision == 0 ? f64_kernel(v) : f32_kernel(v);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, variant_info(precision, v).nt, 0) !=
+        cudaSuccess)
+        nb = 1;
+    if (nb < 1) nb = 1;
+    cache[key] = nb;
+    return nb;
+}
+cudaError_t launch_compute(int precision, int v, int grid, const ComputeArgs &a, cudaStream_t st)
+{
+    return precision == 0 ? launch_f64(v, grid, a, st) : launch_f32(v, grid, a, st);
+}
+}  // namespace sg
+
+using namespace sg;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_errmsg;
+
+static int set_err(int status, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_errmsg = buf;
+    return status;
+}
+
+#define CUDA_TRY(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            return set_err(e_ == cudaErrorMemoryAllocation ? SPHGRAV_ERR_OUT_OF_MEMORY        \
+                                                           : SPHGRAV_ERR_CUDA,                \
+                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,         \
+                           __LINE__);                                                         \
+        }                                                                                     \
+    } while (0)
+
+#define TRY(call)                 \
+    do {                          \
+        int s_ = (call);          \
+        if (s_ != SPHGRAV_OK) return s_; \
+    } while (0)
+
+// ----------------------------------------------------------- device buffers
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    void release()
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct Plan {
+    bool valid = false;
+    // key
+    std::vector<int> offsets;
+    bool full_rows = true;
+    int i_lo = 0, ni = 0, precision = -1, variant = -1;
+    // derived
+    int nsets = 0, ntot = 0, npad_tot = 0, rows_tot = 0, ntiles = 0, nmeta = 0, nitems = 0;
+    int nslots = 0, itile = 0, tj = 0, max_n = 0, max_npad = 0, bits = 21, end_bit = 63;
+    int grid = 1, nchunks_max = 1;
+    std::vector<SetDesc> sets;
+    std::vector<int> tile_set, meta_set;
+    std::vector<WorkItem> items;
+};
+
+struct sphgrav_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+};
+
+struct sphgrav_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    bool capturing = false;
+
+    DBuf<double> in;    // 5 * cap: x y z m range2 (caller order)
+    DBuf<double> out;   // 4 * cap: ax ay az pot (caller order)
+    size_t io_cap = 0;
+    DBuf<unsigned long long> keys_in, keys_out, bbox;
+    DBuf<int> vals_in, vals_out, ilist, nsel, tile_set, meta_set, head, err;
+    DBuf<char> sort_temp, sel_temp;
+    DBuf<double> d64;   // 5 * pcap: x y z m h2 (sorted, padded)
+    DBuf<int> orig;
+    DBuf<unsigned char> flag;
+    DBuf<float> f32;    // 8 * pcap
+    size_t pcap = 0;
+    DBuf<SetDesc> sets;
+    DBuf<ITileMeta> imeta;
+    DBuf<JMeta> jmeta;
+    DBuf<WorkItem> items;
+    DBuf<double> partials, wtile, wdev;
+    DBuf<unsigned long long> kick_counter;
+    DBuf<float> probe_sink;
+
+    PinnedBuf h_in, h_out, h_err;
+    Plan plan;
+
+    // legacy call in flight
+    bool pending = false;
+    int pend_n = 0, pend_i0 = 0, pend_ni = 0;
+    int pend_nsets = 0;
+    double *pend_user[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_start = nullptr, ev_done = nullptr;
+
+    int forced_variant[2] = {-1, -1};
+    std::map<int, std::string> tuned[2];  // N bucket -> variant name
+
+    // kernel timing (sphgrav_profile_*)
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+    size_t prof_used = 0;
+};
+
+template <class T>
+static int ensure(sphgrav_ctx *c, DBuf<T> &b, size_t n, const char *what)
+{
+    if (n <= b.cap && b.p) return SPHGRAV_OK;
+    if (c->capturing)
+        return set_err(SPHGRAV_ERR_PROTOCOL,
+                       "buffer '%s' must grow to %zu elements during a graph capture; call the "
+                       "entry point once with the same sizes before capturing",
+                       what, n);
+    size_t want = std::max<size_t>(n, (size_t)(b.cap * 1.25));
+    if (want == 0) want = 1;
+    b.release();
+    CUDA_TRY(cudaMalloc((void **)&b.p, want * sizeof(T)));
+    b.cap = want;
+    return SPHGRAV_OK;
+}
+
+static int ensure_pinned(sphgrav_ctx *c, PinnedBuf &b, size_t bytes)
+{
+    if (bytes <= b.cap && b.p) return SPHGRAV_OK;
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "host staging cannot grow during capture");
+    size_t want = std::max<size_t>(bytes, (size_t)(b.cap * 1.25));
+    b.release();
+    CUDA_TRY(cudaMallocHost(&b.p, want));
+    b.cap = want;
+    return SPHGRAV_OK;
+}
+
+static int use_device(sphgrav_ctx *c)
+{
+    int cur = -1;
+    CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != c->device) CUDA_TRY(cudaSetDevice(c->device));
+    return SPHGRAV_OK;
+}
+
+// ------------------------------------------------------- variant choice
+static const int kMinChunkJ = 8192;  // shortest j-chunk worth a partial slot
+
+static int ceil_log2(long long v)
+{
+    int b = 0;
+    while ((1ll << b) < v) b++;
+    return b;
+}
+
+static int bucket_of(const std::vector<int> &offsets, bool full_rows, int ni)
+{
+    double s1 = 0.0, s2 = 0.0;
+    for (size_t s = 0; s + 1 < offsets.size(); s++) {
+        double n = offsets[s + 1] - offsets[s];
+        double rows = full_rows ? n : ni;
+        s1 += rows;
+        s2 += rows * n;
+    }
+    double nw = s1 > 0 ? s2 / s1 : 1.0;
+    return (int)std::floor(std::log2(std::max(1.0, nw)));
+}
+
+static int variant_by_name(int precision, const std::string &name)
+{
+    for (int v = 0; v < variant_count(precision); v++)
+        if (name == variant_info(precision, v).name) return v;
+    return -1;
+}
+
+static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> &offsets,
+                          bool full_rows, int ni)
+{
+    if (c->forced_variant[precision] >= 0) return c->forced_variant[precision];
+    const int b = bucket_of(offsets, full_rows, ni);
+    auto it = c->tuned[precision].find(b);
+    if (it != c->tuned[precision].end()) {
+        int v = variant_by_name(precision, it->second);
+        if (v >= 0) return v;
+    }
+    if (precision == SPHGRAV_FP64) return 0;
+    // defaults by pair-weighted mean N: wide i-tiles for large sets, several
+    // threads per row for small ones (more CTAs, shorter tiles per thread)
+    if (b >= 16) return 0;
+    if (b >= 14) return 1;
+    if (b >= 12) return 3;
+    return 4;
+}
+
+// ------------------------------------------------------------------ plan
+static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
+                      int ni, int precision, int variant, Plan &P)
+{
+    const VariantInfo &V = variant_info(precision, variant);
+    P = Plan();
+    P.offsets = offsets;
+    P.full_rows = full_rows;
+    P.i_lo = i_lo;
+    P.ni = ni;
+    P.precision = precision;
+    P.variant = variant;
+    P.nsets = (int)offsets.size() - 1;
+    P.itile = V.itile();
+    P.tj = V.tj;
+    long long poff = 0, ioff = 0, toff = 0, moff = 0;
+    for (int s = 0; s < P.nsets; s++) {
+        SetDesc d;
+        memset(&d, 0, sizeof(d));
+        d.n = offsets[s + 1] - offsets[s];
+        d.off = offsets[s];
+        d.poff = (int)poff;
+        d.npad = (d.n + PAD_J - 1) / PAD_J * PAD_J;
+        d.ioff = (int)ioff;
+        d.ni = full_rows ? d.n : ni;
+        d.i_lo = full_rows ? 0 : i_lo;
+        d.tile_off = (int)toff;
+        d.ntiles = (d.ni + P.itile - 1) / P.itile;
+        d.meta_off = (int)moff;
+        poff += d.npad;
+        ioff += d.ni;
+        toff += d.ntiles;
+        moff += d.npad / META_J;
+        P.max_n = std::max(P.max_n, d.n);
+        P.max_npad = std::max(P.max_npad, d.npad);
+        P.sets.push_back(d);
+    }
+    if (poff > 0x7fffffffll - PAD_J) return set_err(SPHGRAV_ERR_TOO_LARGE, "too many particles");
+    P.ntot = offsets.back() - offsets.front();
+    P.npad_tot = (int)poff;
+    P.rows_tot = (int)ioff;
+    P.ntiles = (int)toff;
+    P.nmeta = (int)moff;
+    const int occ = variant_occupancy(precision, variant);
+    const int resident = occ * c->sm_count;
+    const int target = 4 * resident;
+    int slot = 0;
+    P.nchunks_max = 1;
+    struct Cost { long long cost; WorkItem w; };
+    std::vector<Cost> items;
+    for (int s = 0; s < P.nsets; s++) {
+        SetDesc &d = P.sets[s];
+        const int jtiles = (d.n + P.tj - 1) / P.tj;
+        int nch = P.ntiles > 0 ? (target + P.ntiles - 1) / P.ntiles : 1;
+        const int maxch = std::max(1, (int)(((long long)jtiles * P.tj) / kMinChunkJ));
+        nch = std::max(1, std::min(nch, std::min(maxch, std::max(1, jtiles))));
+        d.nchunks = nch;
+        d.slot_off = slot;
+        slot += d.ntiles * nch;
+        P.nchunks_max = std::max(P.nchunks_max, nch);
+        for (int t = 0; t < d.ntiles; t++) {
+            const int rows = std::min(P.itile, d.ni - t * P.itile);
+            for (int ch = 0; ch < nch; ch++) {
+                WorkItem w;
+                memset(&w, 0, sizeof(w));
+                w.set = s;
+                w.tile = t;
+                w.chunk = ch;
+                w.jb = (int)((long long)jtiles * ch / nch) * P.tj;
+                w.je = (int)((long long)jtiles * (ch + 1) / nch) * P.tj;
+                items.push_back({(long long)rows * (w.je - w.jb), w});
+            }
+        }
+        for (int t = 0; t < d.ntiles; t++) P.tile_set.push_back(s);
+        for (int r = 0; r < d.npad / META_J; r++) P.meta_set.push_back(s);
+    }
+    // longest first: the dynamic queue then balances like LPT scheduling
+    std::stable_sort(items.begin(), items.end(),
+                     [](const Cost &a, const Cost &b) { return a.cost > b.cost; });
+    for (auto &it : items) P.items.push_back(it.w);
+    P.nitems = (int)P.items.size();
+    P.nslots = slot;
+    P.grid = std::max(1, std::min(P.nitems, resident));
+    const int setbits = ceil_log2(std::max(1, P.nsets));
+    P.bits = std::min(21, (64 - setbits) / 3);
+    P.end_bit = 3 * P.bits + setbits;
+    P.valid = true;
+    return SPHGRAV_OK;
+}
+
+static bool plan_matches(const Plan &P, const std::vector<int> &offsets, bool full_rows, int i_lo,
+                         int ni, int precision, int variant)
+{
+    return P.valid && P.offsets == offsets && P.full_rows == full_rows &&
+           (full_rows || (P.i_lo == i_lo && P.ni == ni)) && P.precision == precision &&
+           P.variant == variant;
+}
+
+static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
+                   int ni, int precision, int variant)
+{
+    if (!plan_matches(c->plan, offsets, full_rows, i_lo, ni, precision, variant)) {
+        if (c->capturing)
+            return set_err(SPHGRAV_ERR_PROTOCOL,
+                           "work plan changed during a graph capture; call the entry point once "
+                           "with the same sizes before capturing");
+        Plan P;
+        TRY(build_plan(c, offsets, full_rows, i_lo, ni, precision, variant, P));
+        TRY(ensure(c, c->sets, std::max(1, P.nsets), "sets"));
+        TRY(ensure(c, c->tile_set, std::max(1, P.ntiles), "tile_set"));
+        TRY(ensure(c, c->meta_set, std::max(1, P.nmeta), "meta_set"));
+        TRY(ensure(c, c->items, std::max(1, P.nitems), "items"));
+        CUDA_TRY(cudaMemcpyAsync(c->sets.p, P.sets.data(), sizeof(SetDesc) * P.nsets,
+                                 cudaMemcpyHostToDevice, c->stream));
+        if (P.ntiles)
+            CUDA_TRY(cudaMemcpyAsync(c->tile_set.p, P.tile_set.data(), sizeof(int) * P.ntiles,
+                                     cudaMemcpyHostToDevice, c->stream));
+        if (P.nmeta)
+            CUDA_TRY(cudaMemcpyAsync(c->meta_set.p, P.meta_set.data(), sizeof(int) * P.nmeta,
+                                     cudaMemcpyHostToDevice, c->stream));
+        if (P.nitems)
+            CUDA_TRY(cudaMemcpyAsync(c->items.p, P.items.data(), sizeof(WorkItem) * P.nitems,
+                                     cudaMemcpyHostToDevice, c->stream));
+        // pageable-source copies are staged before return; the vectors may change after
+        c->plan = std::move(P);
+    }
+    const Plan &P = c->plan;
+    const size_t np = std::max(1, P.npad_tot);
+    if (np > c->pcap || !c->d64.p) {
+        TRY(ensure(c, c->d64, 5 * np, "sorted fp64"));
+        TRY(ensure(c, c->orig, np, "orig"));
+        TRY(ensure(c, c->flag, np, "flag"));
+        TRY(ensure(c, c->f32, 8 * np, "sorted f32"));
+        c->pcap = np;
+    }
+    const size_t nt = std::max(1, P.ntot);
+    TRY(ensure(c, c->keys_in, nt, "keys"));
+    TRY(ensure(c, c->keys_out, nt, "keys"));
+    TRY(ensure(c, c->vals_in, nt, "vals"));
+    TRY(ensure(c, c->vals_out, nt, "vals"));
+    TRY(ensure(c, c->ilist, std::max(1, P.rows_tot), "rows"));
+    TRY(ensure(c, c->bbox, 6 * (size_t)std::max(1, P.nsets), "bbox"));
+    TRY(ensure(c, c->imeta, std::max(1, P.ntiles), "itile meta"));
+    TRY(ensure(c, c->jmeta, std::max(1, P.nmeta), "jtile meta"));
+    TRY(ensure(c, c->partials, (size_t)std::max(1, P.nslots) * 4 * P.itile, "partials"));
+    TRY(ensure(c, c->wtile, std::max(1, P.ntiles), "wtile"));
+    TRY(ensure(c, c->wdev, std::max(1, P.nsets), "W"));
+    const size_t sb = sort_temp_bytes(P.ntot, P.end_bit);
+    TRY(ensure(c, c->sort_temp, std::max<size_t>(sb, 1), "sort temp"));
+    if (!P.full_rows) {
+        const size_t selb = select_temp_bytes(P.ntot);
+        TRY(ensure(c, c->sel_temp, std::max<size_t>(selb, 1), "select temp"));
+    }
+    return SPHGRAV_OK;
+}
+
+static SortedF64 sorted64(sphgrav_ctx *c)
+{
+    SortedF64 D;
+    const size_t np = c->pcap;
+    D.x = c->d64.p;
+    D.y = D.x + np;
+    D.z = D.y + np;
+    D.m = D.z + np;
+    D.h2 = D.m + np;
+    D.orig = c->orig.p;
+    D.flag = c->flag.p;
+    return D;
+}
+
+static SortedF32 sorted32(sphgrav_ctx *c)
+{
+    SortedF32 F;
+    const size_t np = c->pcap;
+    F.xh = c->f32.p;
+    F.xl = F.xh + np;
+    F.yh = F.xl + np;
+    F.yl = F.yh + np;
+    F.zh = F.yl + np;
+    F.zl = F.zh + np;
+    F.m = F.zl + np;
+    F.h2 = F.m + np;
+    return F;
+}
+
+// The per-call pipeline on device-resident inputs and outputs.
+static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
+                      int ni, const InputsDev &in, const OutputsDev &out, double *W, int nkernel,
+                      int precision)
+{
+    if (nkernel < 0 || nkernel > 2)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "nkernel must be 0, 1 or 2 (got %d)", nkernel);
+    if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
+    const int variant = choose_variant(c, precision, offsets, full_rows, ni);
+    TRY(prepare(c, offsets, full_rows, i_lo, ni, precision, variant));
+    const Plan &P = c->plan;
+    cudaStream_t st = c->stream;
+    if (P.ntot == 0) return SPHGRAV_OK;
+    SortedF64 D = sorted64(c);
+    SortedF32 F = sorted32(c);
+    CUDA_TRY(launch_validate(in, P.ntot, c->err.p, st));
+    CUDA_TRY(launch_bbox(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, st));
+    CUDA_TRY(launch_morton(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, P.bits, c->keys_in.p,
+                           c->vals_in.p, st));
+    CUDA_TRY(launch_sort(c->sort_temp.p, c->sort_temp.cap, c->keys_in.p, c->keys_out.p,
+                         c->vals_in.p, c->vals_out.p, P.ntot, P.end_bit, st));
+    CUDA_TRY(launch_gather(c->sets.p, P.nsets, P.max_npad, in, c->vals_out.p, D, F, st));
+    if (P.full_rows) {
+        CUDA_TRY(launch_rows_full(c->sets.p, P.nsets, P.max_n, c->ilist.p, st));
+    } else {
+        CUDA_TRY(launch_rows_range(P.sets[0], D, c->ilist.p, c->nsel.p, c->sel_temp.p,
+                                   c->sel_temp.cap, st));
+    }
+    if (precision == SPHGRAV_F32SPLIT) {
+        CUDA_TRY(launch_itile_meta(c->sets.p, P.nsets, P.ntiles, c->tile_set.p, P.itile,
+                                   c->ilist.p, D, c->imeta.p, st));
+        CUDA_TRY(launch_jmeta(c->sets.p, P.nsets, P.nmeta, c->meta_set.p, D, c->jmeta.p, st));
+    }
+    CUDA_TRY(cudaMemsetAsync(c->head.p, 0, sizeof(int), st));
+    ComputeArgs a;
+    a.sets = c->sets.p;
+    a.items = c->items.p;
+    a.nitems = P.nitems;
+    a.head = c->head.p;
+    a.D = D;
+    a.F = F;
+    a.ilist = c->ilist.p;
+    a.imeta = c->imeta.p;
+    a.jmeta = c->jmeta.p;
+    a.partials = c->partials.p;
+    a.err = c->err.p;
+    a.nkernel = nkernel;
+    a.itile = P.itile;
+    const bool timed = c->profiling && !c->capturing && P.nitems > 0;
+    if (timed) {
+        if (c->prof_used == c->prof_events.size()) {
+            cudaEvent_t e0, e1;
+            CUDA_TRY(cudaEventCreate(&e0));
+            CUDA_TRY(cudaEventCreate(&e1));
+            c->prof_events.push_back({e0, e1});
+        }
+        CUDA_TRY(cudaEventRecord(c->prof_events[c->prof_used].first, st));
+    }
+    if (P.nitems > 0) CUDA_TRY(launch_compute(precision, P.variant, P.grid, a, st));
+    if (timed) CUDA_TRY(cudaEventRecord(c->prof_events[c->prof_used++].second, st));
+    CUDA_TRY(launch_merge(c->sets.p, c->tile_set.p, P.ntiles, P.itile, c->ilist.p, D,
+                          c->partials.p, out, c->wtile.p, st));
+    if (W) CUDA_TRY(launch_wsum(c->sets.p, P.nsets, c->wtile.p, W, st));
+    return SPHGRAV_OK;
+}
+
+static int read_device_error(sphgrav_ctx *c)
+{
+    int e = 0;
+    CUDA_TRY(cudaMemcpy(&e, c->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemset(c->err.p, 0, sizeof(int)));
+    if (e & DEVERR_INPUT)
+        return set_err(SPHGRAV_ERR_INVALID_INPUT,
+                       "invalid particle data (mass <= 0, range2 == 0 or a non-finite value)");
+    if (e & DEVERR_TIMEOUT) return set_err(SPHGRAV_ERR_DEVICE_TIMEOUT, "device wait timed out");
+    return SPHGRAV_OK;
+}
+
+// Host-side check of the inputs, the reference's asserts
+// (grav_force_direct.cu:601-602) as a status.
+static int check_host_inputs(int n, const double *x, const double *y, const double *z,
+                             const double *m, const double *r2)
+{
+    for (int i = 0; i < n; i++) {
+        if (!(m[i] > 0.0) || !std::isfinite(m[i]))
+            return set_err(SPHGRAV_ERR_INVALID_INPUT, "mass[%d] = %g must be > 0", i, m[i]);
+        if (r2[i] == 0.0 || !std::isfinite(r2[i]))
+            return set_err(SPHGRAV_ERR_INVALID_INPUT, "range2[%d] = %g must be non-zero", i, r2[i]);
+        if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i]))
+            return set_err(SPHGRAV_ERR_INVALID_INPUT, "position of particle %d is not finite", i);
+    }
+    return SPHGRAV_OK;
+}
+
+// Context-owned input (5 arrays) and output (4 arrays) buffers of io_cap
+// elements each, for the host-buffer entry points and the tuner.
+static int ensure_io(sphgrav_ctx *c, int n)
+{
+    if ((size_t)n > c->io_cap || !c->in.p || !c->out.p) {
+        const size_t want = std::max<size_t>(std::max(n, 1), c->io_cap);
+        TRY(ensure(c, c->in, 5 * want, "inputs"));
+        TRY(ensure(c, c->out, 4 * want, "outputs"));
+        c->io_cap = want;
+    }
+    return SPHGRAV_OK;
+}
+
+// Copy host inputs (length n) to the context's device input buffer.
+static int upload_inputs(sphgrav_ctx *c, int n, const double *x, const double *y, const double *z,
+                         const double *m, const double *r2, InputsDev &in)
+{
+    TRY(ensure_io(c, n));
+    TRY(ensure_pinned(c, c->h_in, 5 * sizeof(double) * std::max(n, 1)));
+    double *h = (double *)c->h_in.p;
+    const double *src[5] = {x, y, z, m, r2};
+    for (int a = 0; a < 5; a++) memcpy(h + (size_t)a * n, src[a], sizeof(double) * n);
+    const size_t cap = c->io_cap;
+    if (n > 0) {
+        // the device buffer holds 5 arrays of io_cap; copy each
+        for (int a = 0; a < 5; a++)
+            CUDA_TRY(cudaMemcpyAsync(c->in.p + a * cap, h + (size_t)a * n, sizeof(double) * n,
+                                     cudaMemcpyHostToDevice, c->stream));
+    }
+    in.x = c->in.p;
+    in.y = in.x + cap;
+    in.z = in.y + cap;
+    in.m = in.z + cap;
+    in.r2 = in.m + cap;
+    return SPHGRAV_OK;
+}
+
+static OutputsDev ctx_outputs(sphgrav_ctx *c)
+{
+    OutputsDev o;
+    const size_t cap = c->io_cap;
+    o.ax = c->out.p;
+    o.ay = o.ax + cap;
+    o.az = o.ay + cap;
+    o.pot = o.az + cap;
+    return o;
+}
+
+// ------------------------------------------------------------ public API
+extern "C" {
+
+const char *sphgrav_status_string(int s)
+{
+    switch (s) {
+    case SPHGRAV_OK: return "ok";
+    case SPHGRAV_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case SPHGRAV_ERR_INVALID_INPUT: return "invalid particle data";
+    case SPHGRAV_ERR_CUDA: return "CUDA error";
+    case SPHGRAV_ERR_NO_DEVICE: return "no CUDA device";
+    case SPHGRAV_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case SPHGRAV_ERR_PROTOCOL: return "call protocol violated";
+    case SPHGRAV_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    case SPHGRAV_ERR_TOO_LARGE: return "size beyond a documented limit";
+    default: return "unknown status";
+    }
+}
+
+const char *sphgrav_last_error_message(void) { return g_errmsg.c_str(); }
+unsigned long long sphgrav_launch_count(void) { return g_launches; }
+
+int sphgrav_variant_count(int precision)
+{
+    if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT) return 0;
+    return variant_count(precision);
+}
+const char *sphgrav_variant_name(int precision, int v)
+{
+    if (v < 0 || v >= sphgrav_variant_count(precision)) return "";
+    return variant_info(precision, v).name;
+}
+
+int sphgrav_create(sphgrav_ctx **out, int device)
+{
+    if (!out) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx pointer is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return set_err(SPHGRAV_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "device %d out of range (%d devices)", device, ndev);
+    CUDA_TRY(cudaSetDevice(device));
+    sphgrav_ctx *c = new sphgrav_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    int st = SPHGRAV_OK;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev_start) != cudaSuccess || cudaEventCreate(&c->ev_done) != cudaSuccess) {
+        st = set_err(SPHGRAV_ERR_CUDA, "stream/event creation failed: %s",
+                     cudaGetErrorString(cudaGetLastError()));
+    }
+    c->stream = c->own_stream;
+    if (st == SPHGRAV_OK) st = ensure(c, c->head, 1, "head");
+    if (st == SPHGRAV_OK) st = ensure(c, c->err, 1, "err");
+    if (st == SPHGRAV_OK) st = ensure(c, c->nsel, 1, "nsel");
+    if (st == SPHGRAV_OK) st = ensure(c, c->kick_counter, 1, "kick counter");
+    if (st == SPHGRAV_OK) st = ensure_pinned(c, c->h_err, sizeof(int));
+    if (st == SPHGRAV_OK && (cudaMemset(c->err.p, 0, sizeof(int)) != cudaSuccess ||
+                             cudaMemset(c->kick_counter.p, 0, sizeof(unsigned long long)) != cudaSuccess))
+        st = set_err(SPHGRAV_ERR_CUDA, "memset failed");
+    if (st != SPHGRAV_OK) {
+        sphgrav_destroy(c);
+        return st;
+    }
+    *out = c;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_destroy(sphgrav_ctx *c)
+{
+    if (!c) return SPHGRAV_OK;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != c->device) cudaSetDevice(c->device);
+    if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+    if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
+    c->in.release(); c->out.release(); c->keys_in.release(); c->keys_out.release();
+    c->bbox.release(); c->vals_in.release(); c->vals_out.release(); c->ilist.release();
+    c->nsel.release(); c->tile_set.release(); c->meta_set.release(); c->head.release();
+    c->err.release(); c->sort_temp.release(); c->sel_temp.release(); c->d64.release();
+    c->orig.release(); c->flag.release(); c->f32.release(); c->sets.release();
+    c->imeta.release(); c->jmeta.release(); c->items.release(); c->partials.release();
+    c->wtile.release(); c->wdev.release(); c->kick_counter.release(); c->probe_sink.release();
+    c->h_in.release(); c->h_out.release(); c->h_err.release();
+    for (auto &e : c->prof_events) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    if (c->ev_start) cudaEventDestroy(c->ev_start);
+    if (c->ev_done) cudaEventDestroy(c->ev_done);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_set_stream(sphgrav_ctx *c, void *stream)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change stream during capture");
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_sync(sphgrav_ctx *c)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    TRY(use_device(c));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
+int sphgrav_forces_device(sphgrav_ctx *c, int n, int i_begin, int ni, const double *x,
+                          const double *y, const double *z, const double *mass,
+                          const double *range2, int nkernel, int precision, double *ax,
+                          double *ay, double *az, double *pot, double *W)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (n < 0 || i_begin < 0 || ni < 0 || i_begin + (long long)ni > n)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad sizes n=%d i_begin=%d ni=%d", n, i_begin, ni);
+    if (n > 0 && (!x || !y || !z || !mass || !range2 || !ax || !ay || !az || !pot))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL data pointer");
+    TRY(use_device(c));
+    std::vector<int> offs = {0, n};
+    const bool full = (i_begin == 0 && ni == n);
+    InputsDev in = {x, y, z, mass, range2};
+    OutputsDev out = {ax, ay, az, pot};
+    if (W && n == 0) CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double), c->stream));
+    return run_device(c, offs, full, i_begin, ni, in, out, W, nkernel, precision);
+}
+
+int sphgrav_batch_forces_device(sphgrav_ctx *c, int nsets, const int *offsets, const double *x,
+                                const double *y, const double *z, const double *mass,
+                                const double *range2, int nkernel, int precision, double *ax,
+                                double *ay, double *az, double *pot, double *W_per_set)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (nsets <= 0 || nsets > MAX_SETS || !offsets)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "nsets must be in [1, %d]", MAX_SETS);
+    std::vector<int> offs(offsets, offsets + nsets + 1);
+    if (offs[0] != 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "offsets[0] must be 0");
+    for (int s = 0; s < nsets; s++)
+        if (offs[s + 1] < offs[s]) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "offsets must not decrease");
+    if (offs.back() > 0 && (!x || !y || !z || !mass || !range2 || !ax || !ay || !az || !pot))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL data pointer");
+    TRY(use_device(c));
+    InputsDev in = {x, y, z, mass, range2};
+    OutputsDev out = {ax, ay, az, pot};
+    return run_device(c, offs, true, 0, 0, in, out, W_per_set, nkernel, precision);
+}
+
+int sphgrav_batch_forces(sphgrav_ctx *c, int nsets, const int *offsets, const double *x,
+                         const double *y, const double *z, const double *mass,
+                         const double *range2, int nkernel, int precision, double *ax, double *ay,
+                         double *az, double *pot, double *W_per_set)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "host-buffer calls cannot be captured");
+    if (nsets <= 0 || nsets > MAX_SETS || !offsets)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "nsets must be in [1, %d]", MAX_SETS);
+    const int n = offsets[nsets];
+    if (offsets[0] != 0 || n < 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad offsets");
+    for (int s = 0; s < nsets; s++)
+        if (offsets[s + 1] < offsets[s]) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "offsets must not decrease");
+    if (n > 0 && (!x || !y || !z || !mass || !range2 || !ax || !ay || !az || !pot))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL data pointer");
+    TRY(use_device(c));
+    TRY(check_host_inputs(n, x, y, z, mass, range2));
+    InputsDev in;
+    TRY(upload_inputs(c, n, x, y, z, mass, range2, in));
+    OutputsDev out = ctx_outputs(c);
+    std::vector<int> offs(offsets, offsets + nsets + 1);
+    TRY(ensure(c, c->wdev, nsets, "W"));
+    TRY(run_device(c, offs, true, 0, 0, in, out, c->wdev.p, nkernel, precision));
+    TRY(ensure_pinned(c, c->h_out, sizeof(double) * (4 * (size_t)n + nsets)));
+    double *h = (double *)c->h_out.p;
+    if (n > 0)
+        for (int q = 0; q < 4; q++)
+            CUDA_TRY(cudaMemcpyAsync(h + (size_t)q * n, c->out.p + (size_t)q * c->io_cap,
+                                     sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(h + 4 * (size_t)n, c->wdev.p, sizeof(double) * nsets,
+                             cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    TRY(read_device_error(c));
+    double *dst[4] = {ax, ay, az, pot};
+    for (int q = 0; q < 4; q++) memcpy(dst[q], h + (size_t)q * n, sizeof(double) * n);
+    if (W_per_set) memcpy(W_per_set, h + 4 * (size_t)n, sizeof(double) * nsets);
+    return SPHGRAV_OK;
+}
+
+int sphgrav_firsthalf(sphgrav_ctx *c, int n, int i_begin, int ni, const double *x, const double *y,
+                      const double *z, const double *mass, const double *range2, int nkernel,
+                      int precision)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "host-buffer calls cannot be captured");
+    if (c->pending)
+        return set_err(SPHGRAV_ERR_PROTOCOL, "firsthalf called twice without lasthalf");
+    if (n < 0 || i_begin < 0 || ni < 0 || i_begin + (long long)ni > n)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad sizes n=%d i_begin=%d ni=%d", n, i_begin, ni);
+    if (n > 0 && (!x || !y || !z || !mass || !range2))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL data pointer");
+    TRY(use_device(c));
+    TRY(check_host_inputs(n, x, y, z, mass, range2));
+    CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
+    InputsDev in;
+    TRY(upload_inputs(c, n, x, y, z, mass, range2, in));
+    OutputsDev out = ctx_outputs(c);
+    std::vector<int> offs = {0, n};
+    const bool full = (i_begin == 0 && ni == n);
+    TRY(run_device(c, offs, full, i_begin, ni, in, out, nullptr, nkernel, precision));
+    TRY(ensure_pinned(c, c->h_out, sizeof(double) * 4 * (size_t)std::max(ni, 1)));
+    double *h = (double *)c->h_out.p;
+    if (ni > 0)
+        for (int q = 0; q < 4; q++)
+            CUDA_TRY(cudaMemcpyAsync(h + (size_t)q * ni, c->out.p + (size_t)q * c->io_cap + i_begin,
+                                     sizeof(double) * ni, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->h_err.p, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev_done, c->stream));
+    c->pending = true;
+    c->pend_n = n;
+    c->pend_i0 = i_begin;
+    c->pend_ni = ni;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_lasthalf(sphgrav_ctx *c, double *ax, double *ay, double *az, double *pot)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (!c->pending) return set_err(SPHGRAV_ERR_PROTOCOL, "lasthalf called without firsthalf");
+    c->pending = false;
+    TRY(use_device(c));
+    CUDA_TRY(cudaEventSynchronize(c->ev_done));
+    const int e = *(int *)c->h_err.p;
+    if (e & DEVERR_INPUT) return set_err(SPHGRAV_ERR_INVALID_INPUT, "invalid particle data");
+    if (e & DEVERR_TIMEOUT) return set_err(SPHGRAV_ERR_DEVICE_TIMEOUT, "device wait timed out");
+    const int ni = c->pend_ni, i0 = c->pend_i0;
+    if (ni > 0 && (!ax || !ay || !az || !pot))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL output pointer");
+    const double *h = (const double *)c->h_out.p;
+    double *dst[4] = {ax, ay, az, pot};
+    for (int q = 0; q < 4; q++) memcpy(dst[q] + i0, h + (size_t)q * ni, sizeof(double) * ni);
+    return SPHGRAV_OK;
+}
+
+int sphgrav_gravforce(sphgrav_ctx *c, int ntot, int ngrav_lower, int ngrav_upper, const double *x,
+                      const double *y, const double *z, const double *am, const double *hp,
+                      const double *u, int nkernel, int precision, double *gx, double *gy,
+                      double *gz, double *grpot)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (ntot < 0 || ngrav_lower < 1 || ngrav_upper < ngrav_lower - 1 || ngrav_upper > ntot)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad row range [%d, %d] of %d", ngrav_lower,
+                       ngrav_upper, ntot);
+    if (ntot > 0 && (!hp || !u)) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL hp or u");
+    std::vector<double> range2(ntot);
+    for (int i = 0; i < ntot; i++) {  // grav.f:15-18
+        range2[i] = 4 * hp[i] * hp[i];
+        if (u[i] == 0.0) range2[i] = -range2[i];
+    }
+    const int len = ngrav_upper - ngrav_lower + 1;  // grav.f:23
+    TRY(sphgrav_firsthalf(c, ntot, ngrav_lower - 1, len, x, y, z, am, range2.data(), nkernel,
+                          precision));
+    return sphgrav_lasthalf(c, gx, gy, gz, grpot);
+}
+
+// ------------------------------------------------------ sweeps & capture
+int sphgrav_kick_positions_device(sphgrav_ctx *c, int n, double *x, double *y, double *z,
+                                  double sigma, unsigned long long seed)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (n < 0 || (n > 0 && (!x || !y || !z)))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad kick arguments");
+    TRY(use_device(c));
+    CUDA_TRY(launch_kick(n, x, y, z, sigma, seed, c->kick_counter.p, c->stream));
+    return SPHGRAV_OK;
+}
+
+int sphgrav_kick_reset(sphgrav_ctx *c, unsigned long long v)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "kick_reset cannot be captured");
+    TRY(use_device(c));
+    CUDA_TRY(cudaMemcpyAsync(c->kick_counter.p, &v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return SPHGRAV_OK;
+}
+
+int sphgrav_capture_begin(sphgrav_ctx *c)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "capture already active");
+    TRY(use_device(c));
+    CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->capturing = true;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_capture_end(sphgrav_ctx *c, sphgrav_graph **out)
+{
+    if (!c || !out) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "no capture active");
+    c->capturing = false;
+    TRY(use_device(c));
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamEndCapture(c->stream, &g));
+    sphgrav_graph *G = new sphgrav_graph();
+    G->graph = g;
+    G->stream = c->stream;
+    G->device = c->device;
+    cudaError_t e = cudaGraphInstantiate(&G->exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        delete G;
+        return set_err(SPHGRAV_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    *out = G;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_graph_launch(sphgrav_graph *G, int repeats)
+{
+    if (!G || repeats < 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad graph launch");
+    for (int r = 0; r < repeats; r++) {
+        CUDA_TRY(cudaGraphLaunch(G->exec, G->stream));
+        ++g_launches;
+    }
+    return SPHGRAV_OK;
+}
+
+int sphgrav_graph_destroy(sphgrav_graph *G)
+{
+    if (!G) return SPHGRAV_OK;
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    delete G;
+    return SPHGRAV_OK;
+}
+
+// ----------------------------------------------------------------- tuning
+int sphgrav_force_variant(sphgrav_ctx *c, int precision, int variant)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
+    if (variant < -1 || variant >= variant_count(precision))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "variant %d out of range", variant);
+    c->forced_variant[precision] = variant;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_autotune(sphgrav_ctx *c, int nsets, const int *offsets, const double *x,
+                     const double *y, const double *z, const double *mass, const double *range2,
+                     int nkernel, int precision)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot tune during capture");
+    if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
+    if (nsets <= 0 || !offsets) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad sets");
+    TRY(use_device(c));
+    const int n = offsets[nsets];
+    TRY(ensure_io(c, n));
+    OutputsDev out = ctx_outputs(c);
+    InputsDev in = {x, y, z, mass, range2};
+    std::vector<int> offs(offsets, offsets + nsets + 1);
+    const int saved = c->forced_variant[precision];
+    float best_ms = 1e30f;
+    int best = -1;
+    for (int v = 0; v < variant_count(precision); v++) {
+        const VariantInfo &V = variant_info(precision, v);
+        if (precision == SPHGRAV_F32SPLIT && !V.newton) continue;  // keeps the precision contract
+        c->forced_variant[precision] = v;
+        int st = run_device(c, offs, true, 0, 0, in, out, nullptr, nkernel, precision);
+        if (st != SPHGRAV_OK) { c->forced_variant[precision] = saved; return st; }
+        float ms_min = 1e30f;
+        for (int r = 0; r < 2; r++) {
+            CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
+            st = run_device(c, offs, true, 0, 0, in, out, nullptr, nkernel, precision);
+            if (st != SPHGRAV_OK) { c->forced_variant[precision] = saved; return st; }
+            CUDA_TRY(cudaEventRecord(c->ev_done, c->stream));
+            CUDA_TRY(cudaEventSynchronize(c->ev_done));
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, c->ev_start, c->ev_done));
+            ms_min = std::min(ms_min, ms);
+        }
+        if (ms_min < best_ms) { best_ms = ms_min; best = v; }
+    }
+    c->forced_variant[precision] = saved;
+    TRY(read_device_error(c));
+    if (best >= 0) c->tuned[precision][bucket_of(offs, true, 0)] = variant_info(precision, best).name;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_tuning_save(sphgrav_ctx *c, const char *path)
+{
+    if (!c || !path) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL argument");
+    FILE *f = fopen(path, "w");
+    if (!f) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "cannot open %s for writing", path);
+    fprintf(f, "{\"format\": \"sphgrav_b200-tuning-1\", \"entries\": [");
+    bool first = true;
+    for (int p = 0; p < 2; p++)
+        for (auto &kv : c->tuned[p]) {
+            fprintf(f, "%s\n  {\"precision\": %d, \"bucket\": %d, \"variant\": \"%s\"}",
+                    first ? "" : ",", p, kv.first, kv.second.c_str());
+            first = false;
+        }
+    fprintf(f, "\n]}\n");
+    fclose(f);
+    return SPHGRAV_OK;
+}
+
+int sphgrav_tuning_load(sphgrav_ctx *c, const char *path)
+{
+    if (!c || !path) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL argument");
+    FILE *f = fopen(path, "r");
+    if (!f) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "cannot open %s", path);
+    std::string s;
+    char buf[4096];
+    size_t k;
+    while ((k = fread(buf, 1, sizeof(buf), f)) > 0) s.append(buf, k);
+    fclose(f);
+    if (s.find("sphgrav_b200-tuning-1") == std::string::npos)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "%s is not a tuning file", path);
+    size_t pos = 0;
+    int loaded = 0;
+    while ((pos = s.find("{\"precision\"", pos)) != std::string::npos) {
+        int p = -1, b = 0;
+        char name[128] = {0};
+        if (sscanf(s.c_str() + pos, "{\"precision\": %d, \"bucket\": %d, \"variant\": \"%127[^\"]\"}",
+                   &p, &b, name) == 3 &&
+            (p == 0 || p == 1) && variant_by_name(p, name) >= 0) {
+            c->tuned[p][b] = name;
+            loaded++;
+        }
+        pos += 12;
+    }
+    (void)loaded;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_last_plan_info(sphgrav_ctx *c, int *nitems, int *nchunks_max, int *variant)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (nitems) *nitems = c->plan.nitems;
+    if (nchunks_max) *nchunks_max = c->plan.nchunks_max;
+    if (variant) *variant = c->plan.variant;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_profile_enable(sphgrav_ctx *c, int on)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    c->profiling = on != 0;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_profile_read(sphgrav_ctx *c, double *kernel_ms, int *launches)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    TRY(use_device(c));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double total = 0.0;
+    for (size_t k = 0; k < c->prof_used; k++) {
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, c->prof_events[k].first, c->prof_events[k].second));
+        total += ms;
+    }
+    if (kernel_ms) *kernel_ms = total;
+    if (launches) *launches = (int)c->prof_used;
+    c->prof_used = 0;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_fp32_peak_probe(sphgrav_ctx *c, int iters, double *tflops)
+{
+    if (!c || !tflops || iters <= 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad probe arguments");
+    TRY(use_device(c));
+    const int blocks = c->sm_count * 8;
+    TRY(ensure(c, c->probe_sink, blocks, "probe"));
+    CUDA_TRY(launch_fp32_probe(std::min(iters, 1000), blocks, c->probe_sink.p, c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
+    CUDA_TRY(launch_fp32_probe(iters, blocks, c->probe_sink.p, c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev_done, c->stream));
+    CUDA_TRY(cudaEventSynchronize(c->ev_done));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, c->ev_start, c->ev_done));
+    const double flops = (double)blocks * 256.0 * iters * 8 * 2 * 2;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return SPHGRAV_OK;
+}
+
+// -------------------------------------------------- legacy Fortran ABI
+static sphgrav_ctx *g_legacy = nullptr;
+static int g_legacy_device = -1;
+static int g_legacy_precision = -1;
+
+static void legacy_fail(const char *where, int st)
+{
+    fprintf(stderr, "sphgrav_b200: %s failed: %s: %s\n", where, sphgrav_status_string(st),
+            sphgrav_last_error_message());
+    abort();
+}
+
+static int legacy_precision()
+{
+    if (g_legacy_precision < 0) {
+        const char *e = getenv("SPHGRAV_PRECISION");
+        g_legacy_precision = (e && (!strcmp(e, "fp64") || !strcmp(e, "FP64"))) ? SPHGRAV_FP64
+                                                                                : SPHGRAV_F32SPLIT;
+    }
+    return g_legacy_precision;
+}
+
+static sphgrav_ctx *legacy_ctx()
+{
+    if (!g_legacy) {
+        int dev = g_legacy_device;
+        if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+        int st = sphgrav_create(&g_legacy, dev);
+        if (st != SPHGRAV_OK) legacy_fail("context creation", st);
+    }
+    return g_legacy;
+}
+
+int sphgrav_legacy_set_precision(int precision)
+{
+    if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
+    g_legacy_precision = precision;
+    return SPHGRAV_OK;
+}
+
+void gpu_init_dev_(int *myrank, double *theta)
+{
+    (void)theta;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        legacy_fail("gpu_init_dev_", set_err(SPHGRAV_ERR_NO_DEVICE, "no CUDA device"));
+    const int dev = myrank ? *myrank : 0;
+    if (dev < 0 || dev >= ndev)
+        legacy_fail("gpu_init_dev_", set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "device %d of %d", dev, ndev));
+    if (g_legacy && g_legacy->device != dev) {
+        sphgrav_destroy(g_legacy);
+        g_legacy = nullptr;
+    }
+    g_legacy_device = dev;
+    if (cudaSetDevice(dev) != cudaSuccess)
+        legacy_fail("gpu_init_dev_", set_err(SPHGRAV_ERR_CUDA, "cudaSetDevice(%d) failed", dev));
+}
+
+void firsthalf_grav_forces_(int *n, int *n_lower, int *my_length, double *px, double *py,
+                            double *pz, double *mass, double *range2, int *q, int *nkernel)
+{
+    (void)q;  // threads per particle: chosen by the library's tuning instead
+    sphgrav_ctx *c = legacy_ctx();
+    int st = sphgrav_firsthalf(c, *n, *n_lower - 1, *my_length, px, py, pz, mass, range2,
+                               *nkernel, legacy_precision());
+    if (st != SPHGRAV_OK) legacy_fail("firsthalf_grav_forces_", st);
+}
+
+void lasthalf_grav_forces_(int *n, double *ax, double *ay, double *az, double *pot, int *myrank)
+{
+    (void)n;
+    (void)myrank;  // never read: the Fortran callers pass five arguments
+    sphgrav_ctx *c = legacy_ctx();
+    int st = sphgrav_lasthalf(c, ax, ay, az, pot);
+    if (st != SPHGRAV_OK) legacy_fail("lasthalf_grav_forces_", st);
+    if (getenv("SPHGRAV_VERBOSE")) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev_start, c->ev_done);
+        fprintf(stderr, " >>> SPHgrav_lib took %g sec\n", ms * 1e-3);
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,363 @@
+// sg_f32.cu -- split-FP32 direct-summation kernel for sm_100a.
+//
+// Per pair (far field, the >99.9% case at large N), in packed f32x2
+// arithmetic so one instruction evaluates two (row, source) pairs:
+//     dr   = x_j' - x_i'                    (tile-relative coordinates)
+//     r2   = dr.dr
+//     y0   = rsqrt.approx(r2), one Newton step  Y = y0 (r2 y0^2 - 3) = -2/r
+//     pot += m_j Y                          (= -2 m_j / r)
+//     acc += (m_j Y)(Y Y) dr                (= -8 m_j dr / r^3)
+// The factors -2 and -8 are exact powers of two removed at the end.
+//
+// Precision design:
+//   * positions arrive as float hi + lo pairs of the FP64 inputs; each CTA
+//     re-expresses its rows and every staged j-tile relative to its i-tile's
+//     centre c:  x' = (x_hi - c_hi) + (x_lo - c_lo).  Near pairs then form
+//     dr without cancellation (error ~ eps * |x - c|, c within the tile),
+//     at a cost of a few flops per staged particle instead of per pair.
+//   * FP32 sums run over one j-tile, then fold into compensated (TwoSum,
+//     "Kahan") float hi/lo accumulators kept in shared memory.
+//   * pairs with r^2 < max(H_i^2, H_j^2) -- the softened near field, where
+//     the reference polynomials cancel by up to ~1e3 near q = 1 -- are
+//     evaluated in FP64 (pair_f64_slots, the CPU-path formulas) and folded
+//     into the same accumulators.  A warp skips the per-pair near test for
+//     a j-tile when the bounding boxes of its rows and of the tile are
+//     farther apart than the largest H of both.
+//   * per (row, j-chunk) results leave the CTA as FP64 partial sums merged
+//     in chunk order (k_merge).
+// Reference kernel replaced: dev_compute_forces / dev_force_ij_nkernel*
+// (parallel_bleeding_edge/src/SPHgrav_lib2/grav_force_direct.cu:55-502).
+#include "sg_launch.h"
+
+namespace sg {
+
+struct TileBox {
+    float lo[3], hi[3];
+    float h2max;
+    int empty;
+};
+
+template <bool NEWTON>
+struct Scales {
+    // accumulated value * scale = physical value
+    static constexpr float acc = NEWTON ? -0.125f : 1.0f;
+    static constexpr float pot = NEWTON ? 0.5f : -1.0f;
+};
+
+__device__ __forceinline__ void geom2(f2 xj, f2 yj, f2 zj, f2 xi, f2 yi, f2 zi, f2 &dx, f2 &dy,
+                                      f2 &dz, f2 &r2)
+{
+    dx = sub2(xj, xi);
+    dy = sub2(yj, yi);
+    dz = sub2(zj, zi);
+    r2 = mul2(dx, dx);
+    r2 = fma2(dy, dy, r2);
+    r2 = fma2(dz, dz, r2);
+}
+
+template <bool NEWTON>
+__device__ __forceinline__ void accum2(f2 dx, f2 dy, f2 dz, f2 r2, f2 mj, f2 &ax, f2 &ay,
+                                       f2 &az, f2 &pp)
+{
+    float ra, rb;
+    upk(r2, ra, rb);
+    const f2 y0 = pk(rsqrt_approx(ra), rsqrt_approx(rb));
+    const f2 ysq = mul2(y0, y0);
+    f2 mr, mr3;
+    if (NEWTON) {
+        const f2 t = fma2(r2, ysq, pk(-3.0f, -3.0f));  // -(3 - r2 y0^2)
+        const f2 yn = mul2(y0, t);                       // -2 y1
+        mr = mul2(mj, yn);                               // -2 m y1
+        const f2 y2 = mul2(yn, yn);                      // 4 y1^2
+        mr3 = mul2(mr, y2);                              // -8 m y1^3
+    } else {
+        mr = mul2(mj, y0);
+        mr3 = mul2(mr, ysq);
+    }
+    ax = fma2(mr3, dx, ax);
+    ay = fma2(mr3, dy, ay);
+    az = fma2(mr3, dz, az);
+    pp = add2(pp, mr);
+}
+
+// Fold a packed FP32 partial into a compensated accumulator pair in shared memory.
+__device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
+{
+    float a, b;
+    upk(v, a, b);
+    float h = *hi, l = *lo;
+    ff_add(h, l, a);
+    ff_add(h, l, b);
+    *hi = h;
+    *lo = l;
+}
+
+template <int NT, int K, int Q, int TJ, bool NEWTON>
+__global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
+{
+    static_assert(TJ % NT == 0 || NT % TJ == 0, "tile/block mismatch");
+    static_assert(TJ % (4 * Q) == 0, "j-tile must hold whole quads per phase");
+    static_assert(32 % Q == 0, "threads per row must divide a warp");
+    constexpr int RPW = 32 / Q;           // row groups per warp
+    constexpr int ITILE = NT * K / Q;     // rows per i-tile
+    constexpr int NMETA = TJ / META_J;
+    constexpr float SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
+
+    __shared__ __align__(16) float s_x[TJ];
+    __shared__ __align__(16) float s_y[TJ];
+    __shared__ __align__(16) float s_z[TJ];
+    __shared__ __align__(16) float s_m[TJ];
+    __shared__ __align__(16) float s_h[TJ];
+    __shared__ float s_acc[K * 8][NT];  // [k*8 + c][tid]: c 0-3 hi (ax ay az pot), 4-7 lo
+    __shared__ TileBox s_box;
+    __shared__ int s_item;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int grp = lane / Q, phase = lane % Q;
+    const SortedF64 D = a.D;
+    const SortedF32 F = a.F;
+
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(a.head, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= a.nitems) break;
+        const WorkItem W = a.items[it];
+        const SetDesc S = a.sets[W.set];
+        const ITileMeta C = a.imeta[S.tile_off + W.tile];
+
+        // rows of this thread
+        int ip[K];
+        bool act[K];
+        f2 xi[K], yi[K], zi[K];
+        float h2i[K];
+        float wlo[3] = {INFINITY, INFINITY, INFINITY}, whi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        float wh2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int li = warp * RPW * K + k * RPW + grp;
+            const int r = W.tile * ITILE + li;
+            act[k] = r < S.ni;
+            ip[k] = act[k] ? a.ilist[S.ioff + r] : 0;
+            float x = 1.0e15f, y = 1.0e15f, z = -1.0e15f, h2 = 0.f;
+            if (act[k]) {
+                const int s = ip[k];
+                x = __fadd_rn(__fsub_rn(F.xh[s], C.chx), __fsub_rn(F.xl[s], C.clx));
+                y = __fadd_rn(__fsub_rn(F.yh[s], C.chy), __fsub_rn(F.yl[s], C.cly));
+                z = __fadd_rn(__fsub_rn(F.zh[s], C.chz), __fsub_rn(F.zl[s], C.clz));
+                h2 = F.h2[s];
+                wlo[0] = fminf(wlo[0], x); whi[0] = fmaxf(whi[0], x);
+                wlo[1] = fminf(wlo[1], y); whi[1] = fmaxf(whi[1], y);
+                wlo[2] = fminf(wlo[2], z); whi[2] = fmaxf(whi[2], z);
+                wh2 = fmaxf(wh2, h2);
+            }
+            xi[k] = pk(x, x);
+            yi[k] = pk(y, y);
+            zi[k] = pk(z, z);
+            h2i[k] = h2;
+#pragma unroll
+            for (int c = 0; c < 8; c++) s_acc[k * 8 + c][tid] = 0.f;
+        }
+        // bounding box of the warp's rows (relative coordinates)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            for (int o = 16; o > 0; o >>= 1) {
+                wlo[d] = fminf(wlo[d], __shfl_xor_sync(0xffffffffu, wlo[d], o));
+                whi[d] = fmaxf(whi[d], __shfl_xor_sync(0xffffffffu, whi[d], o));
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) wh2 = fmaxf(wh2, __shfl_xor_sync(0xffffffffu, wh2, o));
+        const bool warp_rows = wlo[0] <= whi[0];
+        wh2 = wh2 * 1.00001f;
+
+        for (int jt = W.jb; jt < W.je; jt += TJ) {
+            // stage the j-tile relative to the i-tile centre
+            for (int t = tid; t < TJ; t += NT) {
+                const int s = S.poff + jt + t;
+                s_x[t] = __fadd_rn(__fsub_rn(F.xh[s], C.chx), __fsub_rn(F.xl[s], C.clx));
+                s_y[t] = __fadd_rn(__fsub_rn(F.yh[s], C.chy), __fsub_rn(F.yl[s], C.cly));
+                s_z[t] = __fadd_rn(__fsub_rn(F.zh[s], C.chz), __fsub_rn(F.zl[s], C.clz));
+                s_m[t] = F.m[s];
+                s_h[t] = F.h2[s];
+            }
+            if (tid == 0) {
+                TileBox B;
+                B.empty = 1;
+                B.h2max = 0.f;
+                for (int d = 0; d < 3; d++) { B.lo[d] = INFINITY; B.hi[d] = -INFINITY; }
+                const float c3[3] = {C.chx, C.chy, C.chz};
+                for (int r = 0; r < NMETA; r++) {
+                    const JMeta M = a.jmeta[S.meta_off + (jt / META_J) + r];
+                    if (M.ex < 0.f) continue;
+                    B.empty = 0;
+                    const float mc[3] = {M.cx, M.cy, M.cz}, me[3] = {M.ex, M.ey, M.ez};
+                    for (int d = 0; d < 3; d++) {
+                        const float rc = mc[d] - c3[d];
+                        // rounding of the float centres and of the staged
+                        // coordinates: widen by 2^-20 of the magnitudes
+                        const float e = me[d] + 9.5367e-7f * (fabsf(mc[d]) + fabsf(c3[d]) + me[d]);
+                        B.lo[d] = fminf(B.lo[d], rc - e);
+                        B.hi[d] = fmaxf(B.hi[d], rc + e);
+                    }
+                    B.h2max = fmaxf(B.h2max, M.h2max);
+                }
+                s_box = B;
+            }
+            __syncthreads();
+
+            if (warp_rows) {
+                const TileBox B = s_box;
+                bool far = B.empty;
+                if (!far) {
+                    float d2 = 0.f;
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        const float slack = 9.5367e-7f * (fmaxf(fabsf(wlo[d]), fabsf(whi[d])));
+                        float gap = fmaxf(B.lo[d] - whi[d], wlo[d] - B.hi[d]) - slack;
+                        gap = fmaxf(gap, 0.f);
+                        d2 = fmaf(gap, gap, d2);
+                    }
+                    far = d2 > fmaxf(wh2, B.h2max) * 1.0001f;
+                }
+                f2 ax[K], ay[K], az[K], pp[K];
+#pragma unroll
+                for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
+
+                if (far) {
+#pragma unroll 2
+                    for (int qd = phase; qd < TJ / 4; qd += Q) {
+                        const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
+                        const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
+                        const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
+                        const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
+#pragma unroll
+                        for (int k = 0; k < K; k++) {
+                            f2 dx, dy, dz, r2;
+                            geom2(X.x, Y.x, Z.x, xi[k], yi[k], zi[k], dx, dy, dz, r2);
+                            accum2<NEWTON>(dx, dy, dz, r2, M.x, ax[k], ay[k], az[k], pp[k]);
+                            geom2(X.y, Y.y, Z.y, xi[k], yi[k], zi[k], dx, dy, dz, r2);
+                            accum2<NEWTON>(dx, dy, dz, r2, M.y, ax[k], ay[k], az[k], pp[k]);
+                        }
+                    }
+                } else {
+                    for (int qd = phase; qd < TJ / 4; qd += Q) {
+                        const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
+                        const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
+                        const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
+                        const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
+                        const float4 H = *reinterpret_cast<const float4 *>(&s_h[4 * qd]);
+#pragma unroll
+                        for (int k = 0; k < K; k++) {
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                f2 dx, dy, dz, r2;
+                                geom2(h ? X.y : X.x, h ? Y.y : Y.x, h ? Z.y : Z.x, xi[k], yi[k],
+                                      zi[k], dx, dy, dz, r2);
+                                f2 mj = h ? M.y : M.x;
+                                float ra, rb;
+                                upk(r2, ra, rb);
+                                const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
+                                const bool na = ra < fmaxf(h2i[k], ha);
+                                const bool nb = rb < fmaxf(h2i[k], hb);
+                                if (na || nb) {
+                                    const int jp0 = S.poff + jt + 4 * qd + 2 * h;
+                                    float *acc = &s_acc[k * 8][tid];
+                                    if (act[k]) {
+                                        if (na) {
+                                            const PairOut o = pair_f64_slots(D, a.nkernel, ip[k], jp0);
+                                            ff_add_d(acc[0], acc[4 * NT], o.ax / SA);
+                                            ff_add_d(acc[NT], acc[5 * NT], o.ay / SA);
+                                            ff_add_d(acc[2 * NT], acc[6 * NT], o.az / SA);
+                                            ff_add_d(acc[3 * NT], acc[7 * NT], o.pot / SP);
+                                        }
+                                        if (nb) {
+                                            const PairOut o = pair_f64_slots(D, a.nkernel, ip[k], jp0 + 1);
+                                            ff_add_d(acc[0], acc[4 * NT], o.ax / SA);
+                                            ff_add_d(acc[NT], acc[5 * NT], o.ay / SA);
+                                            ff_add_d(acc[2 * NT], acc[6 * NT], o.az / SA);
+                                            ff_add_d(acc[3 * NT], acc[7 * NT], o.pot / SP);
+                                        }
+                                    }
+                                    float ma, mb;
+                                    upk(mj, ma, mb);
+                                    mj = pk(na ? 0.f : ma, nb ? 0.f : mb);
+                                    r2 = pk(na ? 1.f : ra, nb ? 1.f : rb);
+                                }
+                                accum2<NEWTON>(dx, dy, dz, r2, mj, ax[k], ay[k], az[k], pp[k]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    fold(&s_acc[k * 8 + 0][tid], &s_acc[k * 8 + 4][tid], ax[k]);
+                    fold(&s_acc[k * 8 + 1][tid], &s_acc[k * 8 + 5][tid], ay[k]);
+                    fold(&s_acc[k * 8 + 2][tid], &s_acc[k * 8 + 6][tid], az[k]);
+                    fold(&s_acc[k * 8 + 3][tid], &s_acc[k * 8 + 7][tid], pp[k]);
+                }
+            }
+            __syncthreads();
+        }
+
+        // combine the Q threads of a row (fixed order), convert, write FP64 partials
+        double *p = a.partials + (size_t)(S.slot_off + W.tile * S.nchunks + W.chunk) * 4 * ITILE;
+        if (phase == 0) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                if (!act[k]) continue;
+                const int li = warp * RPW * K + k * RPW + grp;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    float h = s_acc[k * 8 + c][tid], l = s_acc[k * 8 + 4 + c][tid];
+                    for (int ph = 1; ph < Q; ph++) {
+                        ff_add(h, l, s_acc[k * 8 + c][tid + ph]);
+                        l = __fadd_rn(l, s_acc[k * 8 + 4 + c][tid + ph]);
+                    }
+                    const double v = ((double)h + (double)l) * (double)(c < 3 ? SA : SP);
+                    p[c * ITILE + li] = v;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+#define SG_F32_VARIANTS(X)                                   \
+    X(256, 4, 1, 256, true, "f32split_nt256_k4_q1_tj256")     \
+    X(256, 2, 1, 256, true, "f32split_nt256_k2_q1_tj256")     \
+    X(128, 4, 1, 256, true, "f32split_nt128_k4_q1_tj256")     \
+    X(256, 2, 2, 256, true, "f32split_nt256_k2_q2_tj256")     \
+    X(256, 1, 4, 256, true, "f32split_nt256_k1_q4_tj256")     \
+    X(128, 2, 1, 128, true, "f32split_nt128_k2_q1_tj128")     \
+    X(256, 4, 1, 256, false, "f32split_nt256_k4_q1_tj256_nonewton")
+
+#define SG_INFO(NT, K, Q, TJ, NW, NAME) {1, NT, K, Q, TJ, NW ? 1 : 0, NAME},
+static const VariantInfo kF32Variants[] = {SG_F32_VARIANTS(SG_INFO)};
+#undef SG_INFO
+#define SG_PTR(NT, K, Q, TJ, NW, NAME) (const void *)k_f32split<NT, K, Q, TJ, NW>,
+static const void *kF32Kernels[] = {SG_F32_VARIANTS(SG_PTR)};
+#undef SG_PTR
+constexpr int kNF32 = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
+
+int f32_variant_count() { return kNF32; }
+const VariantInfo &f32_variant_info(int v) { return kF32Variants[v]; }
+const void *f32_kernel(int v) { return kF32Kernels[v]; }
+
+cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st)
+{
+    int idx = 0;
+#define SG_CASE(NT, K, Q, TJ, NW, NAME)                        \
+    if (v == idx) {                                            \
+        k_f32split<NT, K, Q, TJ, NW><<<grid, NT, 0, st>>>(a);  \
+        ++g_launches;                                          \
+        return cudaGetLastError();                             \
+    }                                                          \
+    ++idx;
+    SG_F32_VARIANTS(SG_CASE)
+#undef SG_CASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace sg

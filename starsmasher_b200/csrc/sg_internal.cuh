@@ -1,0 +1,260 @@
+// sg_internal.cuh -- shared layout, device helpers and the FP64 pair formulas
+// of the B200 gravity library.  Paths in citations are inside the reference
+// project (StarSmasher).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sg {
+
+// ------------------------------------------------------------------ layout
+constexpr int META_J = 64;        // particles per j-tile metadata record
+constexpr int PAD_J = 256;        // per-set padding of the sorted arrays
+constexpr double FAR_POS = 1.0e15;  // position of padding slots (mass 0)
+constexpr int MAX_SETS = 1 << 20;
+
+// One independent particle set (one star model / collision snapshot).
+struct SetDesc {
+    int n;         // particles in the set
+    int off;       // first particle in the caller's concatenated arrays
+    int poff;      // first slot of the set in the padded sorted arrays
+    int npad;      // padded length (multiple of PAD_J)
+    int ioff;      // first entry of the set's rows in the row list
+    int ni;        // rows computed for this set
+    int i_lo;      // rows are set-local original indices [i_lo, i_lo + ni)
+    int tile_off;  // first i-tile of the set (global i-tile index)
+    int ntiles;    // i-tiles of the set
+    int meta_off;  // first j metadata record of the set
+    int slot_off;  // first partial slot of the set (in i-tile partial blocks)
+    int nchunks;   // j-chunks per i-tile
+};
+
+// One unit of the persistent kernels' device-side queue.
+struct WorkItem {
+    int set;     // set index
+    int tile;    // set-local i-tile
+    int jb, je;  // set-local sorted slots [jb, je), multiples of the j-tile
+    int chunk;   // j-chunk index within the i-tile
+    int pad_[3];
+};
+
+// Padded, spatially sorted SoA copies of the inputs.
+struct SortedF64 {
+    double *x, *y, *z, *m, *h2;  // h2 = |range2| = H^2 with H = 2 hp
+    int *orig;                   // global index in the caller's arrays (-1: pad)
+    unsigned char *flag;         // range2 > 0 (the particle has self-potential)
+};
+struct SortedF32 {
+    float *xh, *xl, *yh, *yl, *zh, *zl;  // hi + lo float pairs of the FP64 positions
+    float *m, *h2;
+};
+// Bounding box and largest H^2 of META_J consecutive sorted slots.
+struct JMeta {
+    float cx, cy, cz;   // box centre
+    float ex, ey, ez;   // half extents (negative: no particle)
+    float h2max;
+    float pad_;
+};
+// Centre of an i-tile's bounding box as float hi + lo pairs.
+struct ITileMeta {
+    float chx, chy, chz, clx, cly, clz;
+    float pad_[2];
+};
+
+// Error flag bits written by device code.
+enum : int {
+    DEVERR_INPUT = 1,
+    DEVERR_TIMEOUT = 2,
+};
+
+// Self-potential constants c of the zero-distance rule (cpu_grav.f:141,
+// :252, :359 use c/2 because the triangle adds the self pair twice).
+__host__ __device__ inline double self_c(int nkernel)
+{
+    return nkernel == 0 ? 1.4 : (nkernel == 1 ? 1.9140625 : 1.71875);
+}
+
+// ------------------------------------------------------ FP64 pair formulas
+// Contribution of source j to row i, evaluated from i's side in FP64 with the
+// cpu_grav.f formulas (far: :59-70; near: :71-157 / :187-268 / :298-375).
+// dr = x_j - x_i.  r2 == 0 uses the triangle's zero-distance rule restated
+// per row: i == j gives -c*flag_i*(m/H_i + m/H_j); distinct coincident
+// particles give -c/2 * flag_{lower original index} * (m_j/H_i + m_j/H_j).
+struct PairOut { double ax, ay, az, pot; };
+
+__device__ __forceinline__ void near_kernel_f64(int nkernel, double r2, double rinv,
+                                                double amj, double twohpi, double fourhpi2,
+                                                double twohpj, double fourhpj2,
+                                                double mrinv1, double mrinv3,
+                                                double &gacc, double &gpot)
+{
+    const double invq1 = rinv * twohpi, invq2 = rinv * twohpj;
+    const double qq1 = 1.0 / invq1, qq2 = 1.0 / invq2;
+    const double q21 = qq1 * qq1, q22 = qq2 * qq2;
+    const double mj11 = amj / twohpi, mj12 = amj / twohpj;
+    const double mj21 = mj11 / fourhpi2, mj22 = mj12 / fourhpj2;
+    const double g1 = (r2 <= fourhpi2) ? 1.0 : 0.0;
+    const double g2 = (r2 <= fourhpj2) ? 1.0 : 0.0;
+    double acc1, acc2, pot1, pot2;
+    if (nkernel == 0) {
+        const double q31 = qq1 * q21, q32 = qq2 * q22;
+        const double invq31 = invq1 * invq1 * invq1, invq32 = invq2 * invq2 * invq2;
+        if (qq1 < 0.5) {
+            acc1 = 10.666666666667 + q21 * (32.0 * qq1 - 38.4);
+            pot1 = -2.8 + q21 * (5.333333333333 + q21 * (6.4 * qq1 - 9.6));
+        } else {
+            acc1 = 21.333333333333 - 48.0 * qq1 + 38.4 * q21 - 10.666666666667 * q31
+                 - 0.066666666667 * invq31;
+            pot1 = -3.2 + 0.066666666667 * invq1
+                 + q21 * (10.666666666667 + qq1 * (-16.0 + qq1 * (9.6 - 2.133333333333 * qq1)));
+        }
+        if (qq2 < 0.5) {
+            acc2 = 10.666666666667 + q22 * (32.0 * qq2 - 38.4);
+            pot2 = -2.8 + q22 * (5.333333333333 + q22 * (6.4 * qq2 - 9.6));
+        } else {
+            acc2 = 21.333333333333 - 48.0 * qq2 + 38.4 * q22 - 10.666666666667 * q32
+                 - 0.066666666667 * invq32;
+            pot2 = -3.2 + 0.066666666667 * invq2
+                 + q22 * (10.666666666667 + qq2 * (-16.0 + qq2 * (9.6 - 2.133333333333 * qq2)));
+        }
+        gacc = 0.5 * (g1 * mj21 * acc1 + (1.0 - g1) * mrinv3 + g2 * mj22 * acc2 + (1.0 - g2) * mrinv3);
+        gpot = 0.5 * (g1 * mj11 * pot1 + (g1 - 1.0) * mrinv1 + g2 * mj12 * pot2 + (g2 - 1.0) * mrinv1);
+    } else if (nkernel == 1) {
+        acc1 = 28.4375 + q21 * ((-187.6875) + q21 * (804.375 + q21 * ((-4379.375) + qq1 * (9009.0 + qq1 * ((-8957.8125) + qq1 * (5005.0 + qq1 * ((-1515.9375) + 195.0 * qq1)))))));
+        acc2 = 28.4375 + q22 * ((-187.6875) + q22 * (804.375 + q22 * ((-4379.375) + qq2 * (9009.0 + qq2 * ((-8957.8125) + qq2 * (5005.0 + qq2 * ((-1515.9375) + 195.0 * qq2)))))));
+        pot1 = g1 > 0.0 ? (-3.828125) + q21 * (14.21875 + q21 * ((-46.921875) + q21 * (134.0625 + q21 * ((-547.421875) + qq1 * (1001.0 + qq1 * ((-895.78125) + qq1 * (455.0 + qq1 * ((-126.328125) + 15.0 * qq1)))))))) : 0.0;
+        pot2 = g2 > 0.0 ? (-3.828125) + q22 * (14.21875 + q22 * ((-46.921875) + q22 * (134.0625 + q22 * ((-547.421875) + qq2 * (1001.0 + qq2 * ((-895.78125) + qq2 * (455.0 + qq2 * ((-126.328125) + 15.0 * qq2)))))))) : 0.0;
+        gacc = 0.5 * (g1 * mj21 * acc1 + (1.0 - g1) * mrinv3 + g2 * mj22 * acc2 + (1.0 - g2) * mrinv3);
+        gpot = 0.5 * (mj11 * pot1 + (g1 - 1.0) * mrinv1 + mj12 * pot2 + (g2 - 1.0) * mrinv1);
+    } else {
+        acc1 = 20.625 + q21 * ((-115.5) + q21 * (618.75 + qq1 * ((-1155.0) + qq1 * (962.5 + qq1 * ((-396.0) + 65.625 * qq1)))));
+        acc2 = 20.625 + q22 * ((-115.5) + q22 * (618.75 + qq2 * ((-1155.0) + qq2 * (962.5 + qq2 * ((-396.0) + 65.625 * qq2)))));
+        pot1 = g1 > 0.0 ? (-3.4375) + q21 * (10.3125 + q21 * ((-28.875) + q21 * (103.125 + qq1 * ((-165.0) + qq1 * (120.3125 + qq1 * ((-44.0) + 6.5625 * qq1)))))) : 0.0;
+        pot2 = g2 > 0.0 ? (-3.4375) + q22 * (10.3125 + q22 * ((-28.875) + q22 * (103.125 + qq2 * ((-165.0) + qq2 * (120.3125 + qq2 * ((-44.0) + 6.5625 * qq2)))))) : 0.0;
+        gacc = 0.5 * (g1 * mj21 * acc1 + (1.0 - g1) * mrinv3 + g2 * mj22 * acc2 + (1.0 - g2) * mrinv3);
+        gpot = 0.5 * (mj11 * pot1 + (g1 - 1.0) * mrinv1 + mj12 * pot2 + (g2 - 1.0) * mrinv1);
+    }
+}
+
+// Full FP64 pair from sorted slots ip (row) and jp (source).
+static __device__ __noinline__ PairOut pair_f64_slots(const SortedF64 D, int nkernel, int ip, int jp)
+{
+    const double xi = D.x[ip], yi = D.y[ip], zi = D.z[ip];
+    const double dr1 = D.x[jp] - xi, dr2 = D.y[jp] - yi, dr3 = D.z[jp] - zi;
+    const double r2 = dr1 * dr1 + dr2 * dr2 + dr3 * dr3;
+    const double amj = D.m[jp];
+    const double fourhpi2 = D.h2[ip], fourhpj2 = D.h2[jp];
+    double gacc, gpot;
+    if (r2 >= fmax(fourhpi2, fourhpj2)) {
+        const double rinv = 1.0 / sqrt(r2);
+        const double mrinv1 = rinv * amj;
+        gacc = rinv * rinv * mrinv1;
+        gpot = -mrinv1;
+    } else if (r2 > 0.0) {
+        const double rinv = 1.0 / sqrt(r2);
+        const double mrinv1 = rinv * amj;
+        const double mrinv3 = rinv * rinv * mrinv1;
+        near_kernel_f64(nkernel, r2, rinv, amj, sqrt(fourhpi2), fourhpi2, sqrt(fourhpj2),
+                        fourhpj2, mrinv1, mrinv3, gacc, gpot);
+    } else {
+        gacc = 0.0;
+        const double twohpi = sqrt(fourhpi2), twohpj = sqrt(fourhpj2);
+        const double c = self_c(nkernel);
+        if (ip == jp) {
+            gpot = D.flag[ip] ? -c * (amj / twohpi + amj / twohpj) : 0.0;
+        } else {
+            const int lo = D.orig[ip] < D.orig[jp] ? ip : jp;
+            gpot = D.flag[lo] ? -0.5 * c * (amj / twohpi + amj / twohpj) : 0.0;
+        }
+    }
+    PairOut o;
+    o.ax = gacc * dr1;
+    o.ay = gacc * dr2;
+    o.az = gacc * dr3;
+    o.pot = gpot;
+    return o;
+}
+
+// ----------------------------------------------------- packed FP32 (sm_100)
+// Two FP32 lanes in one 64-bit register; one instruction issues both
+// (add/sub/mul/fma .f32x2, PTX ISA 8.6, sm_100+).
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 pk(float lo, float hi)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk(f2 v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b)
+{
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b)
+{
+    f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b)
+{
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
+{
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Error-free transformation a + b = s + e (Knuth TwoSum).
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e)
+{
+    s = __fadd_rn(a, b);
+    const float bp = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+}
+// Compensated accumulator (hi, lo): add v.
+__device__ __forceinline__ void ff_add(float &hi, float &lo, float v)
+{
+    float s, e;
+    two_sum(hi, v, s, e);
+    hi = s;
+    lo = __fadd_rn(lo, e);
+}
+// Add a double into a compensated float accumulator (hi and lo parts).
+__device__ __forceinline__ void ff_add_d(float &hi, float &lo, double v)
+{
+    const float vh = __double2float_rn(v);
+    const float vl = __double2float_rn(v - (double)vh);
+    ff_add(hi, lo, vh);
+    lo = __fadd_rn(lo, vl);
+}
+
+// Monotone map of doubles to uint64 for atomicMin/atomicMax.
+__device__ __forceinline__ unsigned long long dkey(double v)
+{
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k)
+{
+    unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+}  // namespace sg

@@ -1,0 +1,236 @@
+"""GPU parity tests: the CUDA kernels (through the C-ABI) against the oracle.
+
+Tolerances (per-particle relative errors, particles with |a| < 1e-3 median|a|
+reported separately because cancellation makes their relative error
+ill-conditioned):
+  FP64 kernel      vs CPU-path triangle:  acc <= 1e-12, pot <= 1e-12
+  split-FP32       vs FP64 oracle:        acc <= 1e-6,  pot <= 1e-6
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN_CASES, err_report, load_golden
+from starsmasher_b200 import _lib, api, inputs
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+F32_TOL = 1e-6
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def dev(a):
+    t = _torch()
+    return t.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+@pytest.fixture(scope="module")
+def star16k():
+    return inputs.cached("config1")
+
+
+@pytest.fixture(scope="module")
+def tri16k(star16k):
+    s = star16k
+    return {nk: oracle.triangle(s.x, s.y, s.z, s.m, s.range2, nk) for nk in (0, 1, 2)}
+
+
+@pytest.mark.parametrize("nkernel", [0, 1, 2])
+def test_fp64_matches_cpu_path_config1(gpu_ctx, star16k, tri16k, nkernel):
+    s = star16k
+    ax, ay, az, pot = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, nkernel, "fp64")
+    r = err_report(ax, ay, az, pot, *tri16k[nkernel])
+    print("fp64 vs triangle", nkernel, r)
+    assert r["acc_max"] <= FP64_TOL and r["pot_max"] <= FP64_TOL, r
+    assert r["acc_max_ill"] <= 1e-9, r
+
+
+@pytest.mark.parametrize("nkernel", [0, 1, 2])
+def test_f32split_within_1e6_config1(gpu_ctx, star16k, tri16k, nkernel):
+    s = star16k
+    ax, ay, az, pot = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, nkernel, "f32split")
+    r = err_report(ax, ay, az, pot, *tri16k[nkernel])
+    print("f32split vs triangle", nkernel, r)
+    assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("precision", ["fp64", "f32split"])
+def test_golden_snapshot_potential(gpu_ctx, name, precision):
+    """Reference dumps: stored grpot (FP32-level) reproduced like the oracle does."""
+    d = load_golden(name)
+    ax, ay, az, pot = gpu_ctx.forces(d["x"], d["y"], d["z"], d["am"], d["range2"], 0, precision)
+    rel = np.abs(pot - d["grpot"]) / np.abs(d["grpot"])
+    assert rel.max() < 4e-7
+    o = oracle.rows(d["x"], d["y"], d["z"], d["am"], d["range2"], 0)
+    r = err_report(ax, ay, az, pot, *o)
+    tol = FP64_TOL if precision == "fp64" else F32_TOL
+    assert r["acc_max"] <= tol and r["pot_max"] <= tol, r
+
+
+def test_gravforce_host_mirror_matches(gpu_ctx):
+    """sphgrav_gravforce restates grav.f:15-26 + balAV3.f:418 (hp, u inputs)."""
+    d = load_golden("3stars_start1")
+    u = d["u"].copy()
+    u[::50] = 0.0  # some point masses: negative range2
+    out = gpu_ctx.gravforce(d["x"], d["y"], d["z"], d["am"], d["hp"], u, nkernel=0,
+                            precision="fp64")
+    r2 = 4 * d["hp"] ** 2
+    r2 = np.where(u == 0, -r2, r2)
+    o = oracle.triangle(d["x"], d["y"], d["z"], d["am"], r2, 0)
+    r = err_report(*out, *o)
+    assert r["acc_max"] <= FP64_TOL and r["pot_max"] <= FP64_TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64", "f32split"])
+def test_legacy_abi_row_slice(precision, star16k):
+    """Fortran conventions: 1-based n_lower, only the listed rows written."""
+    s = star16k
+    n = s.n
+    api.gpu_init_dev(0, 0.3)
+    api.set_legacy_precision(precision)
+    lo, length = 3001, 5003  # 1-based first row
+    api.firsthalf_grav_forces(n, lo, length, s.x, s.y, s.z, s.m, s.range2, q=4, nkernel=0)
+    outs = [np.full(n, 7.0) for _ in range(4)]
+    api.lasthalf_grav_forces(n, *outs)
+    rows = np.arange(lo - 1, lo - 1 + length)
+    o = oracle.rows(s.x, s.y, s.z, s.m, s.range2, 0, row_idx=rows)
+    r = err_report(*(a[rows] for a in outs), *o)
+    tol = FP64_TOL if precision == "fp64" else F32_TOL
+    assert r["acc_max"] <= tol and r["pot_max"] <= tol, r
+    mask = np.ones(n, bool)
+    mask[rows] = False
+    for a in outs:
+        assert np.all(a[mask] == 7.0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "f32split"])
+@pytest.mark.parametrize("nkernel", [0, 1, 2])
+def test_edge_cases(gpu_ctx, precision, nkernel):
+    """Coincident particles, point masses, tiny sets, ragged sizes, huge H."""
+    rng = np.random.default_rng(7 + nkernel)
+    cases = []
+    # a few particles, including coincident pairs with different H and mass
+    x = np.array([0.0, 0.0, 0.3, 0.3, 1.0])
+    y = np.array([0.0, 0.0, 0.1, 0.1, -0.2])
+    z = np.zeros(5)
+    m = np.array([1.0, 2.0, 0.5, 0.5, 0.1])
+    r2 = np.array([0.25, 0.0625, 0.04, -0.04, 0.5])
+    cases.append((x, y, z, m, r2))
+    cases.append((np.zeros(1), np.zeros(1), np.zeros(1), np.ones(1), np.ones(1)))
+    cases.append((np.array([0.0, 1.0]), np.zeros(2), np.zeros(2), np.array([1.0, 3.0]),
+                  np.array([4.0, -0.01])))
+    for n in (255, 257, 1029):
+        p = rng.normal(size=(n, 3))
+        mm = rng.uniform(0.1, 1.0, n) / n
+        rr = rng.uniform(0.01, 2.0, n) ** 2
+        rr[::13] *= -1
+        p[5] = p[9]  # a coincident pair
+        cases.append((p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), mm, rr))
+    tol = FP64_TOL if precision == "fp64" else F32_TOL
+    for (x, y, z, m, r2) in cases:
+        got = gpu_ctx.forces(x, y, z, m, r2, nkernel, precision)
+        o = oracle.triangle(x, y, z, m, r2, nkernel)
+        amag = np.sqrt(o[0] ** 2 + o[1] ** 2 + o[2] ** 2)
+        scale = np.maximum(amag, 1e-300)
+        da = np.sqrt((got[0] - o[0]) ** 2 + (got[1] - o[1]) ** 2 + (got[2] - o[2]) ** 2)
+        ok = (da <= tol * scale + 1e-13 * np.max(amag))
+        assert ok.all(), (x.shape[0], np.max(da / scale))
+        np.testing.assert_allclose(got[3], o[3], rtol=tol, atol=0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "f32split"])
+def test_invalid_input_reported(gpu_ctx, precision):
+    x = np.zeros(4)
+    m = np.ones(4)
+    bad = np.ones(4)
+    bad[2] = 0.0
+    with pytest.raises(_lib.SphgravError) as e:
+        gpu_ctx.forces(np.arange(4.0), x, x, m, bad, 0, precision)
+    assert e.value.status == _lib.ERR_INVALID_INPUT
+    m2 = m.copy()
+    m2[1] = -1.0
+    with pytest.raises(_lib.SphgravError) as e:
+        gpu_ctx.forces(np.arange(4.0), x, x, m2, np.ones(4), 0, precision)
+    assert e.value.status == _lib.ERR_INVALID_INPUT
+    # device path: the check runs on the device and is reported at sync
+    t = _torch()
+    dx = dev(np.arange(4.0))
+    dz = dev(x)
+    dm = dev(m2)
+    dr = dev(np.ones(4))
+    outs = [t.zeros(4, dtype=t.float64, device="cuda") for _ in range(4)]
+    gpu_ctx.forces_device(4, dx, dz, dz, dm, dr, *outs, precision=precision)
+    with pytest.raises(_lib.SphgravError) as e:
+        gpu_ctx.sync()
+    assert e.value.status == _lib.ERR_INVALID_INPUT
+    gpu_ctx.sync()  # the flag was cleared
+
+
+def test_protocol_errors(gpu_ctx):
+    with pytest.raises(_lib.SphgravError) as e:
+        _lib.check(gpu_ctx._lib.sphgrav_lasthalf(gpu_ctx._h, None, None, None, None), "lasthalf")
+    assert e.value.status == _lib.ERR_PROTOCOL
+    with pytest.raises(ValueError):
+        gpu_ctx.forces(np.zeros(2), np.zeros(2), np.zeros(2), np.ones(2), np.ones(2), 0, "fp16")
+    with pytest.raises(_lib.SphgravError) as e:
+        gpu_ctx.forces(np.zeros(2), np.zeros(2), np.zeros(2), np.ones(2), np.ones(2), 5)
+    assert e.value.status == _lib.ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("precision", ["fp64", "f32split"])
+def test_deterministic(gpu_ctx, star16k, precision):
+    s = star16k
+    a = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, precision)
+    b = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, precision)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+
+
+def test_every_f32_variant_meets_tolerance(gpu_ctx, star16k, tri16k):
+    s = star16k
+    names = api.variant_names("f32split")
+    try:
+        for v, name in enumerate(names):
+            gpu_ctx.force_variant("f32split", v)
+            got = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
+            r = err_report(*got, *tri16k[0])
+            print(name, r)
+            tol = F32_TOL if "nonewton" not in name else 4 * F32_TOL
+            assert r["acc_max"] <= tol and r["pot_max"] <= tol, (name, r)
+    finally:
+        gpu_ctx.force_variant("f32split", -1)
+
+
+def test_every_fp64_variant_meets_tolerance(gpu_ctx, star16k, tri16k):
+    s = star16k
+    try:
+        for v, name in enumerate(api.variant_names("fp64")):
+            gpu_ctx.force_variant("fp64", v)
+            got = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "fp64")
+            r = err_report(*got, *tri16k[0])
+            assert r["acc_max"] <= FP64_TOL and r["pot_max"] <= FP64_TOL, (name, r)
+    finally:
+        gpu_ctx.force_variant("fp64", -1)
+
+
+def test_red_giant_core_subset(gpu_ctx):
+    """Config-3 physics (core point mass, h and m spanning decades) at
+    N=65,536 on a row subset: split-FP32 within 1e-6 of the FP64 oracle."""
+    s = inputs.red_giant(65536, seed=31)
+    ax, ay, az, pot = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
+    rows = np.concatenate([[0], np.random.default_rng(0).choice(s.n, 3000, replace=False)])
+    o = oracle.rows(s.x, s.y, s.z, s.m, s.range2, 0, row_idx=rows)
+    r = err_report(ax[rows], ay[rows], az[rows], pot[rows], *o)
+    print("red giant 64k", r)
+    assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
+    g = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "fp64")
+    r64 = err_report(*(a[rows] for a in g), *o)
+    assert r64["acc_max"] <= FP64_TOL and r64["pot_max"] <= FP64_TOL, r64

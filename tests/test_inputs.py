@@ -1,0 +1,71 @@
+"""CPU tests of the workload generators and the snapshot reader."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from starsmasher_b200 import inputs
+from starsmasher_b200.snapshot import read_snapshot
+
+
+@pytest.mark.parametrize("n_index,xi1", [(1.0, np.pi), (1.5, 3.65375), (3.0, 6.89685)])
+def test_lane_emden_first_zero(n_index, xi1):
+    _, _, _, got = inputs.lane_emden(n_index)
+    assert got == pytest.approx(xi1, rel=1e-4)
+
+
+def test_polytrope_mass_profile():
+    rng = np.random.default_rng(0)
+    pos, m = inputs.polytrope_equal_mass(rng, 20000, 3.0, 1.0, 1.0)
+    r = np.linalg.norm(pos, axis=1)
+    assert r.max() <= 1.0 + 1e-12
+    assert m.sum() == pytest.approx(1.0)
+    # n=3: half the mass inside ~0.0.28 R (centrally condensed)
+    assert 0.2 < np.median(r) < 0.35
+
+
+def test_knn_smoothing_counts():
+    rng = np.random.default_rng(1)
+    pos = rng.random((3000, 3))
+    r2 = inputs.knn_range2(pos, 64)
+    i = 17
+    d2 = np.sum((pos - pos[i]) ** 2, axis=1)
+    assert np.sum(d2 < r2[i] * (1 - 1e-12)) == 64  # 64 others + itself strictly inside
+    assert np.sum(d2 <= r2[i]) == 65
+
+
+def test_red_giant_spans():
+    s = inputs.red_giant(20000, seed=3)
+    assert s.m[0] == 0.3 and s.range2[0] == pytest.approx(-0.01)
+    gas_m = s.m[1:]
+    assert gas_m.max() / gas_m.min() == pytest.approx(1e4, rel=1e-6)
+    assert s.m.sum() == pytest.approx(1.0)
+    h = np.sqrt(s.range2[1:])
+    assert h.max() / h.min() > 100  # ~1e3 at N=1M; fewer particles -> smaller span
+
+
+def test_batch_and_snapshots_shapes():
+    b = inputs.batch_models(5, 256, 1024, seed=4)
+    assert b.nsets == 5 and b.offsets[0] == 0 and np.all(np.diff(b.offsets) >= 256)
+    for s in range(b.nsets):
+        a, e = b.offsets[s], b.offsets[s + 1]
+        assert b.m[a:e].sum() == pytest.approx(1.0)
+    c = inputs.collision_snapshots(3, 1000, 2000, seed=5)
+    assert c.nsets == 3
+    com = [np.sum(c.m[a:e] * c.x[a:e]) / np.sum(c.m[a:e])
+           for a, e in zip(c.offsets[:-1], c.offsets[1:])]
+    assert np.max(np.abs(com)) < 0.05
+
+
+REF_SNAP = "/root/reference/example_input/3_stars/sph.start1u"
+
+
+def test_snapshot_reader_roundtrip_against_fixture():
+    g = np.load(os.path.join(ROOT, "tests", "golden", "snap_3stars_start1.npz"))
+    if os.path.exists(REF_SNAP):
+        s = read_snapshot(REF_SNAP)
+        assert s.ntot == 4944
+        for k in ("x", "y", "z", "am", "hp", "u", "grpot"):
+            np.testing.assert_array_equal(s.data[k], g[k])
+    assert g["x"].shape == (4944,)
