@@ -132,12 +132,16 @@ def cpu_baseline(ws, target_s: float, rank_seed_rows: int = 0):
         a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
         n = b - a
         x, y, z, m, r2 = (arr[a:b] for arr in (ws.x, ws.y, ws.z, ws.m, ws.range2))
-        # calibrate on a short slice in the middle of the triangle
+        # calibrate on a slice in the middle of the triangle (>= 0.3 s of work)
         lo = n // 3
         rows = max(threads, min(n - lo, 2 * threads))
-        t0 = time.perf_counter()
-        oracle.triangle(x, y, z, m, r2, 0, lo, lo + rows, threads)
-        dt = time.perf_counter() - t0
+        while True:
+            t0 = time.perf_counter()
+            oracle.triangle(x, y, z, m, r2, 0, lo, lo + rows, threads)
+            dt = time.perf_counter() - t0
+            if dt >= 0.3 or lo + rows >= n or dt >= target_s:
+                break
+            rows = min(n - lo, int(rows * max(2.0, 0.4 / max(dt, 1e-3))))
         evals = sum(n - i for i in range(lo, lo + rows))
         rate = evals / max(dt, 1e-9)
         want = max(0.0, target_s - total_t) * rate
@@ -163,7 +167,12 @@ def cpu_baseline(ws, target_s: float, rank_seed_rows: int = 0):
 
 
 def load_workload(name: str, rank: int):
+    """configN (the five benchmark workloads) or polytrope:N (one equal-mass
+    n=3 polytrope of N particles, for small profiling cases)."""
     from starsmasher_b200 import inputs
+    if name.startswith("polytrope:"):
+        n = int(name.split(":")[1])
+        return inputs.single_polytrope(n, 3.0, seed=10 + 100 * rank)
     seed = {"config1": 1, "config2": 2, "config3": 3, "config4": 4, "config5": 5}[name] + 100 * rank
     return inputs.cached(name, seed=seed)
 
@@ -224,7 +233,9 @@ def main():
     pairs = ws.pairs
     batched = ws.nsets > 1
 
-    stream = torch.cuda.current_stream()
+    # one dedicated stream for the library, the L2 flush and the timing events
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
     ctx = Context(device)
     ctx.set_stream(stream.cuda_stream)
 

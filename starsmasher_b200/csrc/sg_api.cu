@@ -30,6 +30,8 @@ cudaError_t launch_f64(int v, int grid, const ComputeArgs &a, cudaStream_t st);
 int f32_variant_count();
 const VariantInfo &f32_variant_info(int v);
 const void *f32_kernel(int v);
+int f32_smem_bytes(int v);
+cudaError_t f32_prepare(int v);
 cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st);
 
 int variant_count(int precision) { return precision == 0 ? f64_variant_count() : f32_variant_count(); }
@@ -45,7 +47,12 @@ int variant_occupancy(int precision, int v)
     if (it != cache.end()) return it->second;
     int nb = 0;
     const void *k = precision == 0 ? f64_kernel(v) : f32_kernel(v);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, variant_info(precision, v).nt, 0) !=
+    size_t dyn = 0;
+    if (precision == 1) {
+        f32_prepare(v);
+        dyn = (size_t)f32_smem_bytes(v);
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, variant_info(precision, v).nt, dyn) !=
         cudaSuccess)
         nb = 1;
     if (nb < 1) nb = 1;

@@ -9,14 +9,22 @@
 //     acc += (m_j Y)(Y Y) dr                (= -8 m_j dr / r^3)
 // The factors -2 and -8 are exact powers of two removed at the end.
 //
+// Data movement: each j-tile (TJ sources) arrives in shared memory by 1-D
+// bulk async copies (cp.async.bulk, the TMA engine; no multicast) of its SoA
+// arrays x_hi, x_lo, y_hi, y_lo, z_hi, z_lo, m, H^2 and of its bounding-box
+// records, double-buffered: tile k+1 is in flight while tile k is summed.
+// One elected thread issues the copies; completion is an mbarrier
+// transaction count, waited on with a bounded poll.
+//
 // Precision design:
 //   * positions arrive as float hi + lo pairs of the FP64 inputs; each CTA
 //     re-expresses its rows and every staged j-tile relative to its i-tile's
-//     centre c:  x' = (x_hi - c_hi) + (x_lo - c_lo).  Near pairs then form
-//     dr without cancellation (error ~ eps * |x - c|, c within the tile),
-//     at a cost of a few flops per staged particle instead of per pair.
-//   * FP32 sums run over one j-tile, then fold into compensated (TwoSum,
-//     "Kahan") float hi/lo accumulators kept in shared memory.
+//     centre c:  x' = (x_hi - c_hi) + (x_lo - c_lo),  a few flops per staged
+//     particle instead of per pair.
+//   * acceleration sums run in FP32 over sub-blocks of 8 sources per lane,
+//     are added into a per-tile FP32 sum, which folds into compensated
+//     (TwoSum, "Kahan") float hi/lo accumulators in shared memory once per
+//     tile; the potential (terms of one sign) folds per tile directly.
 //   * pairs with r^2 < max(H_i^2, H_j^2) -- the softened near field, where
 //     the reference polynomials cancel by up to ~1e3 near q = 1 -- are
 //     evaluated in FP64 (pair_f64_slots, the CPU-path formulas) and folded
@@ -92,25 +100,59 @@ __device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
     *lo = l;
 }
 
+// Near-field pair (r^2 < max H^2) in FP64, folded into the row's
+// compensated accumulators acc[c * stride] (hi) / acc[(4 + c) * stride] (lo),
+// in the accumulators' scaled units.
+template <bool NEWTON>
+__device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, int jp, float *acc,
+                                       int stride)
+{
+    constexpr double SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
+    const PairOut o = pair_f64_slots(D, nkernel, ip, jp);
+    ff_add_d(acc[0], acc[4 * stride], o.ax / SA);
+    ff_add_d(acc[stride], acc[5 * stride], o.ay / SA);
+    ff_add_d(acc[2 * stride], acc[6 * stride], o.az / SA);
+    ff_add_d(acc[3 * stride], acc[7 * stride], o.pot / SP);
+}
+
+// Shared-memory layout of one CTA (dynamic shared memory).
+template <int NT, int K, int TJ>
+struct F32Smem {
+    static constexpr int NMETA = TJ / META_J;
+    static constexpr int RAW = 0;                               // [2][8][TJ] floats
+    static constexpr int META = RAW + 2 * 8 * TJ * 4;           // [2][NMETA] JMeta
+    static constexpr int COMP = META + 2 * NMETA * 32;          // [5][TJ] floats
+    static constexpr int ACC = COMP + 5 * TJ * 4;               // [K*8][NT] floats
+    static constexpr int BOX = ACC + K * 8 * NT * 4;            // TileBox
+    static constexpr int BAR = BOX + 64;                        // 2 mbarriers
+    static constexpr int ITEM = BAR + 16;
+    static constexpr int BYTES = ITEM + 16;
+    static constexpr uint32_t TX = 8 * TJ * 4 + NMETA * 32;     // bytes per tile
+};
+
 template <int NT, int K, int Q, int TJ, bool NEWTON>
 __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
 {
     static_assert(TJ % NT == 0 || NT % TJ == 0, "tile/block mismatch");
-    static_assert(TJ % (4 * Q) == 0, "j-tile must hold whole quads per phase");
     static_assert(32 % Q == 0, "threads per row must divide a warp");
-    constexpr int RPW = 32 / Q;           // row groups per warp
-    constexpr int ITILE = NT * K / Q;     // rows per i-tile
-    constexpr int NMETA = TJ / META_J;
+    constexpr int SUBQ = 4;                    // quads per sub-block (8 sources per lane)
+    static_assert((TJ / 4) % (Q * SUBQ) == 0, "j-tile must hold whole sub-blocks");
+    constexpr int RPW = 32 / Q;                // row groups per warp
+    constexpr int ITILE = NT * K / Q;          // rows per i-tile
+    using L = F32Smem<NT, K, TJ>;
+    constexpr int NMETA = L::NMETA;
     constexpr float SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
+    constexpr uint32_t WAIT_LIMIT = 1u << 22;
 
-    __shared__ __align__(16) float s_x[TJ];
-    __shared__ __align__(16) float s_y[TJ];
-    __shared__ __align__(16) float s_z[TJ];
-    __shared__ __align__(16) float s_m[TJ];
-    __shared__ __align__(16) float s_h[TJ];
-    __shared__ float s_acc[K * 8][NT];  // [k*8 + c][tid]: c 0-3 hi (ax ay az pot), 4-7 lo
-    __shared__ TileBox s_box;
-    __shared__ int s_item;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *raw = reinterpret_cast<float *>(smem + L::RAW);
+    JMeta *s_meta = reinterpret_cast<JMeta *>(smem + L::META);
+    float *s_x = reinterpret_cast<float *>(smem + L::COMP);
+    float *s_y = s_x + TJ, *s_z = s_y + TJ, *s_m = s_z + TJ, *s_h = s_m + TJ;
+    float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
+    TileBox *s_box = reinterpret_cast<TileBox *>(smem + L::BOX);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::BAR);
+    int *s_item = reinterpret_cast<int *>(smem + L::ITEM);
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -118,17 +160,41 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
     const SortedF64 D = a.D;
     const SortedF32 F = a.F;
 
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t uses[2] = {0u, 0u};  // completed phases per buffer (same in every thread)
+    bool pending[2] = {false, false};  // copies in flight per buffer (issuing thread only)
+    bool failed = false;
+
+    // issue the bulk copies of tile slots [s0, s0+TJ) of set S into buffer b
+    auto issue = [&](const SetDesc &S, int jt, int b) {
+        float *dst = raw + b * 8 * TJ;
+        const int s0 = S.poff + jt;
+        pending[b] = true;
+        mbar_arrive_expect_tx(&bar[b], L::TX);
+        const float *src[8] = {F.xh, F.xl, F.yh, F.yl, F.zh, F.zl, F.m, F.h2};
+#pragma unroll
+        for (int k = 0; k < 8; k++) bulk_g2s(dst + k * TJ, src[k] + s0, TJ * 4, &bar[b]);
+        bulk_g2s(s_meta + b * NMETA, a.jmeta + S.meta_off + jt / META_J, NMETA * 32, &bar[b]);
+    };
+
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.head, 1);
+        if (tid == 0) *s_item = atomicAdd(a.head, 1);
         __syncthreads();
-        const int it = s_item;
+        const int it = *s_item;
         __syncthreads();
-        if (it >= a.nitems) break;
+        if (it >= a.nitems || failed) break;
         const WorkItem W = a.items[it];
         const SetDesc S = a.sets[W.set];
         const ITileMeta C = a.imeta[S.tile_off + W.tile];
+        const int ntile = (W.je - W.jb) / TJ;
+        if (tid == 0 && ntile > 0) issue(S, W.jb, (uses[0] + uses[1]) & 1);
 
-        // rows of this thread
+        // rows of this thread, relative to the i-tile centre
         int ip[K];
         bool act[K];
         f2 xi[K], yi[K], zi[K];
@@ -158,9 +224,8 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
             zi[k] = pk(z, z);
             h2i[k] = h2;
 #pragma unroll
-            for (int c = 0; c < 8; c++) s_acc[k * 8 + c][tid] = 0.f;
+            for (int c = 0; c < 8; c++) s_acc[(k * 8 + c) * NT + tid] = 0.f;
         }
-        // bounding box of the warp's rows (relative coordinates)
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             for (int o = 16; o > 0; o >>= 1) {
@@ -172,15 +237,28 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
         const bool warp_rows = wlo[0] <= whi[0];
         wh2 = wh2 * 1.00001f;
 
-        for (int jt = W.jb; jt < W.je; jt += TJ) {
-            // stage the j-tile relative to the i-tile centre
-            for (int t = tid; t < TJ; t += NT) {
-                const int s = S.poff + jt + t;
-                s_x[t] = __fadd_rn(__fsub_rn(F.xh[s], C.chx), __fsub_rn(F.xl[s], C.clx));
-                s_y[t] = __fadd_rn(__fsub_rn(F.yh[s], C.chy), __fsub_rn(F.yl[s], C.cly));
-                s_z[t] = __fadd_rn(__fsub_rn(F.zh[s], C.chz), __fsub_rn(F.zl[s], C.clz));
-                s_m[t] = F.m[s];
-                s_h[t] = F.h2[s];
+        for (int t = 0; t < ntile; t++) {
+            const int jt = W.jb + t * TJ;
+            const int b = (uses[0] + uses[1]) & 1;
+            // prefetch the next tile into the other buffer (its previous
+            // contents were consumed before the last __syncthreads)
+            if (tid == 0 && t + 1 < ntile) issue(S, jt + TJ, b ^ 1);
+            if (!mbar_wait_bounded(&bar[b], uses[b] & 1, WAIT_LIMIT)) {
+                if (tid == 0) atomicOr(a.err, DEVERR_TIMEOUT);
+                failed = true;
+            }
+            if (__syncthreads_or(failed)) { failed = true; break; }
+            uses[b]++;
+            pending[b] = false;
+
+            // transform: tile-relative float coordinates
+            const float *rb = raw + b * 8 * TJ;
+            for (int j = tid; j < TJ; j += NT) {
+                s_x[j] = __fadd_rn(__fsub_rn(rb[j], C.chx), __fsub_rn(rb[TJ + j], C.clx));
+                s_y[j] = __fadd_rn(__fsub_rn(rb[2 * TJ + j], C.chy), __fsub_rn(rb[3 * TJ + j], C.cly));
+                s_z[j] = __fadd_rn(__fsub_rn(rb[4 * TJ + j], C.chz), __fsub_rn(rb[5 * TJ + j], C.clz));
+                s_m[j] = rb[6 * TJ + j];
+                s_h[j] = rb[7 * TJ + j];
             }
             if (tid == 0) {
                 TileBox B;
@@ -188,8 +266,9 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
                 B.h2max = 0.f;
                 for (int d = 0; d < 3; d++) { B.lo[d] = INFINITY; B.hi[d] = -INFINITY; }
                 const float c3[3] = {C.chx, C.chy, C.chz};
+#pragma unroll
                 for (int r = 0; r < NMETA; r++) {
-                    const JMeta M = a.jmeta[S.meta_off + (jt / META_J) + r];
+                    const JMeta M = s_meta[b * NMETA + r];
                     if (M.ex < 0.f) continue;
                     B.empty = 0;
                     const float mc[3] = {M.cx, M.cy, M.cz}, me[3] = {M.ex, M.ey, M.ez};
@@ -203,12 +282,12 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
                     }
                     B.h2max = fmaxf(B.h2max, M.h2max);
                 }
-                s_box = B;
+                *s_box = B;
             }
             __syncthreads();
 
             if (warp_rows) {
-                const TileBox B = s_box;
+                const TileBox B = *s_box;
                 bool far = B.empty;
                 if (!far) {
                     float d2 = 0.f;
@@ -221,85 +300,98 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
                     }
                     far = d2 > fmaxf(wh2, B.h2max) * 1.0001f;
                 }
-                f2 ax[K], ay[K], az[K], pp[K];
+                // tile sums: acceleration two-level (sub-block -> tile), potential one level
+                f2 tx[K], ty[K], tz[K], pp[K];
 #pragma unroll
-                for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
+                for (int k = 0; k < K; k++) tx[k] = ty[k] = tz[k] = pp[k] = pk(0.f, 0.f);
 
                 if (far) {
-#pragma unroll 2
-                    for (int qd = phase; qd < TJ / 4; qd += Q) {
-                        const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
-                        const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
-                        const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
-                        const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
+                    for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
+                        f2 ax[K], ay[K], az[K];
+#pragma unroll
+                        for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pk(0.f, 0.f);
+#pragma unroll
+                        for (int s = 0; s < SUBQ; s++) {
+                            const int qd = base + s * Q;
+                            const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
+                            const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
+                            const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
+                            const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
+#pragma unroll
+                            for (int k = 0; k < K; k++) {
+                                f2 dx, dy, dz, r2;
+                                geom2(X.x, Y.x, Z.x, xi[k], yi[k], zi[k], dx, dy, dz, r2);
+                                accum2<NEWTON>(dx, dy, dz, r2, M.x, ax[k], ay[k], az[k], pp[k]);
+                                geom2(X.y, Y.y, Z.y, xi[k], yi[k], zi[k], dx, dy, dz, r2);
+                                accum2<NEWTON>(dx, dy, dz, r2, M.y, ax[k], ay[k], az[k], pp[k]);
+                            }
+                        }
 #pragma unroll
                         for (int k = 0; k < K; k++) {
-                            f2 dx, dy, dz, r2;
-                            geom2(X.x, Y.x, Z.x, xi[k], yi[k], zi[k], dx, dy, dz, r2);
-                            accum2<NEWTON>(dx, dy, dz, r2, M.x, ax[k], ay[k], az[k], pp[k]);
-                            geom2(X.y, Y.y, Z.y, xi[k], yi[k], zi[k], dx, dy, dz, r2);
-                            accum2<NEWTON>(dx, dy, dz, r2, M.y, ax[k], ay[k], az[k], pp[k]);
+                            tx[k] = add2(tx[k], ax[k]);
+                            ty[k] = add2(ty[k], ay[k]);
+                            tz[k] = add2(tz[k], az[k]);
                         }
                     }
                 } else {
-                    for (int qd = phase; qd < TJ / 4; qd += Q) {
-                        const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
-                        const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
-                        const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
-                        const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
-                        const float4 H = *reinterpret_cast<const float4 *>(&s_h[4 * qd]);
+                    for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
+                        f2 ax[K], ay[K], az[K];
+#pragma unroll
+                        for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pk(0.f, 0.f);
+                        for (int s = 0; s < SUBQ; s++) {
+                            const int qd = base + s * Q;
+                            const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
+                            const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
+                            const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
+                            const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
+                            const float4 H = *reinterpret_cast<const float4 *>(&s_h[4 * qd]);
+#pragma unroll
+                            for (int k = 0; k < K; k++) {
+#pragma unroll
+                                for (int h = 0; h < 2; h++) {
+                                    f2 dx, dy, dz, r2;
+                                    geom2(h ? X.y : X.x, h ? Y.y : Y.x, h ? Z.y : Z.x, xi[k], yi[k],
+                                          zi[k], dx, dy, dz, r2);
+                                    f2 mj = h ? M.y : M.x;
+                                    float ra, rb;
+                                    upk(r2, ra, rb);
+                                    const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
+                                    const bool na = ra < fmaxf(h2i[k], ha);
+                                    const bool nb = rb < fmaxf(h2i[k], hb);
+                                    if (na || nb) {
+                                        const int jp0 = S.poff + jt + 4 * qd + 2 * h;
+                                        float *acc = s_acc + (k * 8) * NT + tid;
+                                        if (act[k] && na) near_fold<NEWTON>(D, a.nkernel, ip[k], jp0, acc, NT);
+                                        if (act[k] && nb) near_fold<NEWTON>(D, a.nkernel, ip[k], jp0 + 1, acc, NT);
+                                        float ma, mb;
+                                        upk(mj, ma, mb);
+                                        mj = pk(na ? 0.f : ma, nb ? 0.f : mb);
+                                        r2 = pk(na ? 1.f : ra, nb ? 1.f : rb);
+                                    }
+                                    accum2<NEWTON>(dx, dy, dz, r2, mj, ax[k], ay[k], az[k], pp[k]);
+                                }
+                            }
+                        }
 #pragma unroll
                         for (int k = 0; k < K; k++) {
-#pragma unroll
-                            for (int h = 0; h < 2; h++) {
-                                f2 dx, dy, dz, r2;
-                                geom2(h ? X.y : X.x, h ? Y.y : Y.x, h ? Z.y : Z.x, xi[k], yi[k],
-                                      zi[k], dx, dy, dz, r2);
-                                f2 mj = h ? M.y : M.x;
-                                float ra, rb;
-                                upk(r2, ra, rb);
-                                const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
-                                const bool na = ra < fmaxf(h2i[k], ha);
-                                const bool nb = rb < fmaxf(h2i[k], hb);
-                                if (na || nb) {
-                                    const int jp0 = S.poff + jt + 4 * qd + 2 * h;
-                                    float *acc = &s_acc[k * 8][tid];
-                                    if (act[k]) {
-                                        if (na) {
-                                            const PairOut o = pair_f64_slots(D, a.nkernel, ip[k], jp0);
-                                            ff_add_d(acc[0], acc[4 * NT], o.ax / SA);
-                                            ff_add_d(acc[NT], acc[5 * NT], o.ay / SA);
-                                            ff_add_d(acc[2 * NT], acc[6 * NT], o.az / SA);
-                                            ff_add_d(acc[3 * NT], acc[7 * NT], o.pot / SP);
-                                        }
-                                        if (nb) {
-                                            const PairOut o = pair_f64_slots(D, a.nkernel, ip[k], jp0 + 1);
-                                            ff_add_d(acc[0], acc[4 * NT], o.ax / SA);
-                                            ff_add_d(acc[NT], acc[5 * NT], o.ay / SA);
-                                            ff_add_d(acc[2 * NT], acc[6 * NT], o.az / SA);
-                                            ff_add_d(acc[3 * NT], acc[7 * NT], o.pot / SP);
-                                        }
-                                    }
-                                    float ma, mb;
-                                    upk(mj, ma, mb);
-                                    mj = pk(na ? 0.f : ma, nb ? 0.f : mb);
-                                    r2 = pk(na ? 1.f : ra, nb ? 1.f : rb);
-                                }
-                                accum2<NEWTON>(dx, dy, dz, r2, mj, ax[k], ay[k], az[k], pp[k]);
-                            }
+                            tx[k] = add2(tx[k], ax[k]);
+                            ty[k] = add2(ty[k], ay[k]);
+                            tz[k] = add2(tz[k], az[k]);
                         }
                     }
                 }
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    fold(&s_acc[k * 8 + 0][tid], &s_acc[k * 8 + 4][tid], ax[k]);
-                    fold(&s_acc[k * 8 + 1][tid], &s_acc[k * 8 + 5][tid], ay[k]);
-                    fold(&s_acc[k * 8 + 2][tid], &s_acc[k * 8 + 6][tid], az[k]);
-                    fold(&s_acc[k * 8 + 3][tid], &s_acc[k * 8 + 7][tid], pp[k]);
+                    float *acc = s_acc + (k * 8) * NT + tid;
+                    fold(acc, acc + 4 * NT, tx[k]);
+                    fold(acc + NT, acc + 5 * NT, ty[k]);
+                    fold(acc + 2 * NT, acc + 6 * NT, tz[k]);
+                    fold(acc + 3 * NT, acc + 7 * NT, pp[k]);
                 }
             }
             __syncthreads();
         }
+        if (failed) break;
 
         // combine the Q threads of a row (fixed order), convert, write FP64 partials
         double *p = a.partials + (size_t)(S.slot_off + W.tile * S.nchunks + W.chunk) * 4 * ITILE;
@@ -310,10 +402,10 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
                 const int li = warp * RPW * K + k * RPW + grp;
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    float h = s_acc[k * 8 + c][tid], l = s_acc[k * 8 + 4 + c][tid];
+                    float h = s_acc[(k * 8 + c) * NT + tid], l = s_acc[(k * 8 + 4 + c) * NT + tid];
                     for (int ph = 1; ph < Q; ph++) {
-                        ff_add(h, l, s_acc[k * 8 + c][tid + ph]);
-                        l = __fadd_rn(l, s_acc[k * 8 + 4 + c][tid + ph]);
+                        ff_add(h, l, s_acc[(k * 8 + c) * NT + tid + ph]);
+                        l = __fadd_rn(l, s_acc[(k * 8 + 4 + c) * NT + tid + ph]);
                     }
                     const double v = ((double)h + (double)l) * (double)(c < 3 ? SA : SP);
                     p[c * ITILE + li] = v;
@@ -322,15 +414,21 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
         }
         __syncthreads();
     }
+    // never leave with bulk copies in flight into this CTA's shared memory:
+    // a copy is outstanding iff a buffer was issued and not yet waited for
+    if (failed && tid == 0) {
+        for (int b = 0; b < 2; b++)
+            if (pending[b]) mbar_wait_bounded(&bar[b], uses[b] & 1, WAIT_LIMIT);
+    }
 }
 
 #define SG_F32_VARIANTS(X)                                   \
     X(256, 4, 1, 256, true, "f32split_nt256_k4_q1_tj256")     \
     X(256, 2, 1, 256, true, "f32split_nt256_k2_q1_tj256")     \
     X(128, 4, 1, 256, true, "f32split_nt128_k4_q1_tj256")     \
+    X(128, 2, 1, 256, true, "f32split_nt128_k2_q1_tj256")     \
     X(256, 2, 2, 256, true, "f32split_nt256_k2_q2_tj256")     \
     X(256, 1, 4, 256, true, "f32split_nt256_k1_q4_tj256")     \
-    X(128, 2, 1, 128, true, "f32split_nt128_k2_q1_tj128")     \
     X(256, 4, 1, 256, false, "f32split_nt256_k4_q1_tj256_nonewton")
 
 #define SG_INFO(NT, K, Q, TJ, NW, NAME) {1, NT, K, Q, TJ, NW ? 1 : 0, NAME},
@@ -339,21 +437,39 @@ static const VariantInfo kF32Variants[] = {SG_F32_VARIANTS(SG_INFO)};
 #define SG_PTR(NT, K, Q, TJ, NW, NAME) (const void *)k_f32split<NT, K, Q, TJ, NW>,
 static const void *kF32Kernels[] = {SG_F32_VARIANTS(SG_PTR)};
 #undef SG_PTR
+#define SG_SMEM(NT, K, Q, TJ, NW, NAME) F32Smem<NT, K, TJ>::BYTES,
+static const int kF32Smem[] = {SG_F32_VARIANTS(SG_SMEM)};
+#undef SG_SMEM
 constexpr int kNF32 = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
 
 int f32_variant_count() { return kNF32; }
 const VariantInfo &f32_variant_info(int v) { return kF32Variants[v]; }
 const void *f32_kernel(int v) { return kF32Kernels[v]; }
+int f32_smem_bytes(int v) { return kF32Smem[v]; }
+
+// Opt in to more than 48 KB of dynamic shared memory (once per variant).
+cudaError_t f32_prepare(int v)
+{
+    static bool done[kNF32] = {};
+    if (v < 0 || v >= kNF32) return cudaErrorInvalidValue;
+    if (done[v]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kF32Kernels[v], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kF32Smem[v]);
+    if (e == cudaSuccess) done[v] = true;
+    return e;
+}
 
 cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st)
 {
+    cudaError_t e = f32_prepare(v);
+    if (e != cudaSuccess) return e;
     int idx = 0;
-#define SG_CASE(NT, K, Q, TJ, NW, NAME)                        \
-    if (v == idx) {                                            \
-        k_f32split<NT, K, Q, TJ, NW><<<grid, NT, 0, st>>>(a);  \
-        ++g_launches;                                          \
-        return cudaGetLastError();                             \
-    }                                                          \
+#define SG_CASE(NT, K, Q, TJ, NW, NAME)                                                \
+    if (v == idx) {                                                                    \
+        k_f32split<NT, K, Q, TJ, NW><<<grid, NT, F32Smem<NT, K, TJ>::BYTES, st>>>(a);  \
+        ++g_launches;                                                                  \
+        return cudaGetLastError();                                                     \
+    }                                                                                  \
     ++idx;
     SG_F32_VARIANTS(SG_CASE)
 #undef SG_CASE
