@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--variant", type=int, default=-1,
+                   help="force a kernel variant of --precision (default: tuned/automatic)")
     return p.parse_args()
 
 
@@ -238,6 +240,8 @@ def main():
     torch.cuda.set_stream(stream)
     ctx = Context(device)
     ctx.set_stream(stream.cuda_stream)
+    if args.variant >= 0:
+        ctx.force_variant(args.precision, args.variant)
 
     dt = torch.float64
     X = [torch.as_tensor(a).to(device=f"cuda:{device}", dtype=dt)

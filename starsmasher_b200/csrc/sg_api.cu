@@ -226,7 +226,7 @@ static int use_device(sphgrav_ctx *c)
 }
 
 // ------------------------------------------------------- variant choice
-static const int kMinChunkJ = 8192;  // shortest j-chunk worth a partial slot
+static const int kMinChunkJ = 2048;  // shortest j-chunk worth a partial slot
 
 static int ceil_log2(long long v)
 {
@@ -268,9 +268,8 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     if (precision == SPHGRAV_FP64) return 0;
     // defaults by pair-weighted mean N: wide i-tiles for large sets, several
     // threads per row for small ones (more CTAs, shorter tiles per thread)
-    if (b >= 16) return 0;
-    if (b >= 14) return 1;
-    if (b >= 12) return 3;
+    if (b >= 15) return 0;
+    if (b >= 13) return 3;
     return 4;
 }
 

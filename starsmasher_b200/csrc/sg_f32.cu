@@ -9,30 +9,37 @@
 //     acc += (m_j Y)(Y Y) dr                (= -8 m_j dr / r^3)
 // The factors -2 and -8 are exact powers of two removed at the end.
 //
-// Data movement: each j-tile (TJ sources) arrives in shared memory by 1-D
-// bulk async copies (cp.async.bulk, the TMA engine; no multicast) of its SoA
-// arrays x_hi, x_lo, y_hi, y_lo, z_hi, z_lo, m, H^2 and of its bounding-box
-// records, double-buffered: tile k+1 is in flight while tile k is summed.
-// One elected thread issues the copies; completion is an mbarrier
-// transaction count, waited on with a bounded poll.
+// CTA organisation (warp-specialised, persistent over a device queue of
+// (set, i-tile, j-chunk) items):
+//   * one producer warp: issues 1-D bulk async copies (cp.async.bulk, the
+//     TMA engine; no multicast) of each j-tile's SoA arrays x_hi, x_lo, y_hi,
+//     y_lo, z_hi, z_lo, m, H^2 and bounding-box records into a double-
+//     buffered raw area, waits for their mbarrier transaction count, rewrites
+//     the tile as i-tile-relative floats into an NS-stage ring and signals
+//     the stage "full";
+//   * W consumer warps: each owns 32*K/Q rows in registers, waits for a full
+//     stage, sums the tile, and signals it "empty".  Consumers never meet at
+//     a CTA-wide barrier inside an item, so warps that hit near-field pairs
+//     may run behind the others by up to NS-1 tiles.
+//   * every mbarrier wait is a bounded poll; a timeout sets an error bit and
+//     the CTA leaves at the next item boundary after its copies have landed.
 //
 // Precision design:
-//   * positions arrive as float hi + lo pairs of the FP64 inputs; each CTA
-//     re-expresses its rows and every staged j-tile relative to its i-tile's
-//     centre c:  x' = (x_hi - c_hi) + (x_lo - c_lo),  a few flops per staged
-//     particle instead of per pair.
-//   * acceleration sums run in FP32 over sub-blocks of 8 sources per lane,
-//     are added into a per-tile FP32 sum, which folds into compensated
-//     (TwoSum, "Kahan") float hi/lo accumulators in shared memory once per
-//     tile; the potential (terms of one sign) folds per tile directly.
+//   * positions arrive as float hi + lo pairs of the FP64 inputs; rows and
+//     staged sources are re-expressed relative to the i-tile's centre c:
+//     x' = (x_hi - c_hi) + (x_lo - c_lo), a few flops per staged particle
+//     instead of per pair.
+//   * sums run in FP32 over sub-blocks of 8 sources per lane, are added into
+//     a per-tile FP32 sum that folds into compensated (TwoSum, "Kahan") float
+//     hi/lo accumulators in shared memory once per tile.
 //   * pairs with r^2 < max(H_i^2, H_j^2) -- the softened near field, where
 //     the reference polynomials cancel by up to ~1e3 near q = 1 -- are
 //     evaluated in FP64 (pair_f64_slots, the CPU-path formulas) and folded
 //     into the same accumulators.  A warp skips the per-pair near test for
-//     a j-tile when the bounding boxes of its rows and of the tile are
-//     farther apart than the largest H of both.
-//   * per (row, j-chunk) results leave the CTA as FP64 partial sums merged
-//     in chunk order (k_merge).
+//     a tile when the bounding boxes of its rows and of the tile are farther
+//     apart than the largest H of both.
+//   * per (row, j-chunk) results leave the CTA as FP64 partial sums merged in
+//     chunk order (k_merge).
 // Reference kernel replaced: dev_compute_forces / dev_force_ij_nkernel*
 // (parallel_bleeding_edge/src/SPHgrav_lib2/grav_force_direct.cu:55-502).
 #include "sg_launch.h"
@@ -115,31 +122,33 @@ __device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, i
     ff_add_d(acc[3 * stride], acc[7 * stride], o.pot / SP);
 }
 
-// Shared-memory layout of one CTA (dynamic shared memory).
-template <int NT, int K, int TJ>
-struct F32Smem {
+// Shared-memory layout of one CTA (dynamic shared memory, byte offsets).
+template <int W, int K, int TJ, int NS>
+struct WsSmem {
+    static constexpr int NT = W * 32;
     static constexpr int NMETA = TJ / META_J;
-    static constexpr int RAW = 0;                               // [2][8][TJ] floats
-    static constexpr int META = RAW + 2 * 8 * TJ * 4;           // [2][NMETA] JMeta
-    static constexpr int COMP = META + 2 * NMETA * 32;          // [5][TJ] floats
-    static constexpr int ACC = COMP + 5 * TJ * 4;               // [K*8][NT] floats
-    static constexpr int BOX = ACC + K * 8 * NT * 4;            // TileBox
-    static constexpr int BAR = BOX + 64;                        // 2 mbarriers
-    static constexpr int ITEM = BAR + 16;
+    static constexpr int RAW = 0;                          // [2][8][TJ] floats (TMA targets)
+    static constexpr int META = RAW + 2 * 8 * TJ * 4;      // [2][NMETA] JMeta (TMA targets)
+    static constexpr int COMP = META + 2 * NMETA * 32;     // [NS][5][TJ] floats
+    static constexpr int BOX = COMP + NS * 5 * TJ * 4;     // [NS] TileBox
+    static constexpr int ACC = BOX + NS * 32;              // [K*8][NT] floats
+    static constexpr int BAR = ACC + K * 8 * NT * 4;       // 2 + 2*NS mbarriers
+    static constexpr int ITEM = BAR + (2 + 2 * NS) * 8;    // 2 ints
     static constexpr int BYTES = ITEM + 16;
-    static constexpr uint32_t TX = 8 * TJ * 4 + NMETA * 32;     // bytes per tile
+    static constexpr uint32_t TX = 8 * TJ * 4 + NMETA * 32;  // bytes per tile
 };
 
-template <int NT, int K, int Q, int TJ, bool NEWTON>
-__global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
+template <int W, int K, int Q, int TJ, int NS, bool NEWTON>
+__global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 {
-    static_assert(TJ % NT == 0 || NT % TJ == 0, "tile/block mismatch");
     static_assert(32 % Q == 0, "threads per row must divide a warp");
-    constexpr int SUBQ = 4;                    // quads per sub-block (8 sources per lane)
+    constexpr int SUBQ = 4;                // quads per sub-block (8 sources per lane)
     static_assert((TJ / 4) % (Q * SUBQ) == 0, "j-tile must hold whole sub-blocks");
-    constexpr int RPW = 32 / Q;                // row groups per warp
-    constexpr int ITILE = NT * K / Q;          // rows per i-tile
-    using L = F32Smem<NT, K, TJ>;
+    static_assert(TJ % 32 == 0, "producer lanes split the tile");
+    using L = WsSmem<W, K, TJ, NS>;
+    constexpr int NT = L::NT;              // consumer threads
+    constexpr int RPW = 32 / Q;            // row groups per warp
+    constexpr int ITILE = NT * K / Q;      // rows per i-tile
     constexpr int NMETA = L::NMETA;
     constexpr float SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
     constexpr uint32_t WAIT_LIMIT = 1u << 22;
@@ -147,297 +156,335 @@ __global__ void __launch_bounds__(NT) k_f32split(ComputeArgs a)
     extern __shared__ __align__(128) unsigned char smem[];
     float *raw = reinterpret_cast<float *>(smem + L::RAW);
     JMeta *s_meta = reinterpret_cast<JMeta *>(smem + L::META);
-    float *s_x = reinterpret_cast<float *>(smem + L::COMP);
-    float *s_y = s_x + TJ, *s_z = s_y + TJ, *s_m = s_z + TJ, *s_h = s_m + TJ;
-    float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
+    float *comp = reinterpret_cast<float *>(smem + L::COMP);
     TileBox *s_box = reinterpret_cast<TileBox *>(smem + L::BOX);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::BAR);
-    int *s_item = reinterpret_cast<int *>(smem + L::ITEM);
+    float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
+    uint64_t *bar_raw = reinterpret_cast<uint64_t *>(smem + L::BAR);  // [2]
+    uint64_t *bar_full = bar_raw + 2;                                  // [NS]
+    uint64_t *bar_empty = bar_full + NS;                               // [NS]
+    int *s_item = reinterpret_cast<int *>(smem + L::ITEM);             // [2]
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
+    const bool producer = (warp == W);
     const int grp = lane / Q, phase = lane % Q;
     const SortedF64 D = a.D;
     const SortedF32 F = a.F;
 
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        mbar_init(&bar_raw[0], 1);
+        mbar_init(&bar_raw[1], 1);
+        for (int s = 0; s < NS; s++) {
+            mbar_init(&bar_full[s], 32);   // every producer lane arrives
+            mbar_init(&bar_empty[s], NT);  // every consumer thread arrives
+        }
         fence_mbar_init();
     }
     __syncthreads();
-    uint32_t uses[2] = {0u, 0u};  // completed phases per buffer (same in every thread)
-    bool pending[2] = {false, false};  // copies in flight per buffer (issuing thread only)
-    bool failed = false;
 
-    // issue the bulk copies of tile slots [s0, s0+TJ) of set S into buffer b
-    auto issue = [&](const SetDesc &S, int jt, int b) {
+    uint32_t g = 0;                        // tiles this CTA has passed through its ring
+    bool failed = false;
+    bool pending[2] = {false, false};      // producer lane 0: raw copies in flight
+    uint32_t pend_par[2] = {0u, 0u};       // ... and the barrier phase they complete
+
+    // bulk copies of set-local slots [jt, jt+TJ) (ring tile gt) into raw buffer gt & 1
+    auto issue = [&](const SetDesc &S, int jt, uint32_t gt) {
+        const int b = gt & 1;
         float *dst = raw + b * 8 * TJ;
         const int s0 = S.poff + jt;
         pending[b] = true;
-        mbar_arrive_expect_tx(&bar[b], L::TX);
+        pend_par[b] = (gt >> 1) & 1;
+        fence_mbar_init();  // order earlier generic reads of the buffer before the async writes
+        mbar_arrive_expect_tx(&bar_raw[b], L::TX);
         const float *src[8] = {F.xh, F.xl, F.yh, F.yl, F.zh, F.zl, F.m, F.h2};
 #pragma unroll
-        for (int k = 0; k < 8; k++) bulk_g2s(dst + k * TJ, src[k] + s0, TJ * 4, &bar[b]);
-        bulk_g2s(s_meta + b * NMETA, a.jmeta + S.meta_off + jt / META_J, NMETA * 32, &bar[b]);
+        for (int k = 0; k < 8; k++) bulk_g2s(dst + k * TJ, src[k] + s0, TJ * 4, &bar_raw[b]);
+        bulk_g2s(s_meta + b * NMETA, a.jmeta + S.meta_off + jt / META_J, NMETA * 32, &bar_raw[b]);
     };
 
-    for (;;) {
-        if (tid == 0) *s_item = atomicAdd(a.head, 1);
-        __syncthreads();
-        const int it = *s_item;
-        __syncthreads();
-        if (it >= a.nitems || failed) break;
-        const WorkItem W = a.items[it];
-        const SetDesc S = a.sets[W.set];
-        const ITileMeta C = a.imeta[S.tile_off + W.tile];
-        const int ntile = (W.je - W.jb) / TJ;
-        if (tid == 0 && ntile > 0) issue(S, W.jb, (uses[0] + uses[1]) & 1);
+    for (int iter = 0;; iter++) {
+        if (tid == 0) s_item[iter & 1] = atomicAdd(a.head, 1);
+        if (__syncthreads_or(failed)) break;
+        const int it = s_item[iter & 1];
+        if (it >= a.nitems) break;
+        const WorkItem Wk = a.items[it];
+        const SetDesc S = a.sets[Wk.set];
+        const ITileMeta C = a.imeta[S.tile_off + Wk.tile];
+        const int ntile = (Wk.je - Wk.jb) / TJ;
 
-        // rows of this thread, relative to the i-tile centre
-        int ip[K];
-        bool act[K];
-        f2 xi[K], yi[K], zi[K];
-        float h2i[K];
-        float wlo[3] = {INFINITY, INFINITY, INFINITY}, whi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        float wh2 = 0.f;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            const int li = warp * RPW * K + k * RPW + grp;
-            const int r = W.tile * ITILE + li;
-            act[k] = r < S.ni;
-            ip[k] = act[k] ? a.ilist[S.ioff + r] : 0;
-            float x = 1.0e15f, y = 1.0e15f, z = -1.0e15f, h2 = 0.f;
-            if (act[k]) {
-                const int s = ip[k];
-                x = __fadd_rn(__fsub_rn(F.xh[s], C.chx), __fsub_rn(F.xl[s], C.clx));
-                y = __fadd_rn(__fsub_rn(F.yh[s], C.chy), __fsub_rn(F.yl[s], C.cly));
-                z = __fadd_rn(__fsub_rn(F.zh[s], C.chz), __fsub_rn(F.zl[s], C.clz));
-                h2 = F.h2[s];
-                wlo[0] = fminf(wlo[0], x); whi[0] = fmaxf(whi[0], x);
-                wlo[1] = fminf(wlo[1], y); whi[1] = fmaxf(whi[1], y);
-                wlo[2] = fminf(wlo[2], z); whi[2] = fmaxf(whi[2], z);
-                wh2 = fmaxf(wh2, h2);
-            }
-            xi[k] = pk(x, x);
-            yi[k] = pk(y, y);
-            zi[k] = pk(z, z);
-            h2i[k] = h2;
-#pragma unroll
-            for (int c = 0; c < 8; c++) s_acc[(k * 8 + c) * NT + tid] = 0.f;
-        }
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            for (int o = 16; o > 0; o >>= 1) {
-                wlo[d] = fminf(wlo[d], __shfl_xor_sync(0xffffffffu, wlo[d], o));
-                whi[d] = fmaxf(whi[d], __shfl_xor_sync(0xffffffffu, whi[d], o));
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) wh2 = fmaxf(wh2, __shfl_xor_sync(0xffffffffu, wh2, o));
-        const bool warp_rows = wlo[0] <= whi[0];
-        wh2 = wh2 * 1.00001f;
-
-        for (int t = 0; t < ntile; t++) {
-            const int jt = W.jb + t * TJ;
-            const int b = (uses[0] + uses[1]) & 1;
-            // prefetch the next tile into the other buffer (its previous
-            // contents were consumed before the last __syncthreads)
-            if (tid == 0 && t + 1 < ntile) issue(S, jt + TJ, b ^ 1);
-            if (!mbar_wait_bounded(&bar[b], uses[b] & 1, WAIT_LIMIT)) {
-                if (tid == 0) atomicOr(a.err, DEVERR_TIMEOUT);
-                failed = true;
-            }
-            if (__syncthreads_or(failed)) { failed = true; break; }
-            uses[b]++;
-            pending[b] = false;
-
-            // transform: tile-relative float coordinates
-            const float *rb = raw + b * 8 * TJ;
-            for (int j = tid; j < TJ; j += NT) {
-                s_x[j] = __fadd_rn(__fsub_rn(rb[j], C.chx), __fsub_rn(rb[TJ + j], C.clx));
-                s_y[j] = __fadd_rn(__fsub_rn(rb[2 * TJ + j], C.chy), __fsub_rn(rb[3 * TJ + j], C.cly));
-                s_z[j] = __fadd_rn(__fsub_rn(rb[4 * TJ + j], C.chz), __fsub_rn(rb[5 * TJ + j], C.clz));
-                s_m[j] = rb[6 * TJ + j];
-                s_h[j] = rb[7 * TJ + j];
-            }
-            if (tid == 0) {
-                TileBox B;
-                B.empty = 1;
-                B.h2max = 0.f;
-                for (int d = 0; d < 3; d++) { B.lo[d] = INFINITY; B.hi[d] = -INFINITY; }
-                const float c3[3] = {C.chx, C.chy, C.chz};
-#pragma unroll
-                for (int r = 0; r < NMETA; r++) {
-                    const JMeta M = s_meta[b * NMETA + r];
-                    if (M.ex < 0.f) continue;
-                    B.empty = 0;
-                    const float mc[3] = {M.cx, M.cy, M.cz}, me[3] = {M.ex, M.ey, M.ez};
-                    for (int d = 0; d < 3; d++) {
-                        const float rc = mc[d] - c3[d];
-                        // rounding of the float centres and of the staged
-                        // coordinates: widen by 2^-20 of the magnitudes
-                        const float e = me[d] + 9.5367e-7f * (fabsf(mc[d]) + fabsf(c3[d]) + me[d]);
-                        B.lo[d] = fminf(B.lo[d], rc - e);
-                        B.hi[d] = fmaxf(B.hi[d], rc + e);
-                    }
-                    B.h2max = fmaxf(B.h2max, M.h2max);
+        if (producer) {
+            // ------------------------------------------------ producer warp
+            if (lane == 0 && ntile > 0) issue(S, Wk.jb, g);
+            for (int t = 0; t < ntile && !failed; t++) {
+                const uint32_t gt = g + t;
+                const int rb = gt & 1;
+                const int s = gt % NS;
+                if (lane == 0 && t + 1 < ntile) issue(S, Wk.jb + (t + 1) * TJ, gt + 1);
+                bool ok = mbar_wait_bounded(&bar_raw[rb], (gt >> 1) & 1, WAIT_LIMIT);
+                if (ok && lane == 0) pending[rb] = false;
+                ok = ok && mbar_wait_bounded(&bar_empty[s], ((gt / NS) & 1) ^ 1, WAIT_LIMIT);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(a.err, DEVERR_TIMEOUT);
+                    failed = true;
+                    break;
                 }
-                *s_box = B;
+                // rewrite the tile relative to the i-tile centre
+                const float *rbuf = raw + rb * 8 * TJ;
+                float *cx = comp + s * 5 * TJ;
+#pragma unroll 4
+                for (int j = lane; j < TJ; j += 32) {
+                    cx[j] = __fadd_rn(__fsub_rn(rbuf[j], C.chx), __fsub_rn(rbuf[TJ + j], C.clx));
+                    cx[TJ + j] = __fadd_rn(__fsub_rn(rbuf[2 * TJ + j], C.chy),
+                                           __fsub_rn(rbuf[3 * TJ + j], C.cly));
+                    cx[2 * TJ + j] = __fadd_rn(__fsub_rn(rbuf[4 * TJ + j], C.chz),
+                                               __fsub_rn(rbuf[5 * TJ + j], C.clz));
+                    cx[3 * TJ + j] = rbuf[6 * TJ + j];
+                    cx[4 * TJ + j] = rbuf[7 * TJ + j];
+                }
+                if (lane == 0) {
+                    TileBox B;
+                    B.empty = 1;
+                    B.h2max = 0.f;
+                    for (int d = 0; d < 3; d++) { B.lo[d] = INFINITY; B.hi[d] = -INFINITY; }
+                    const float c3[3] = {C.chx, C.chy, C.chz};
+#pragma unroll
+                    for (int r = 0; r < NMETA; r++) {
+                        const JMeta M = s_meta[rb * NMETA + r];
+                        if (M.ex < 0.f) continue;
+                        B.empty = 0;
+                        const float mc[3] = {M.cx, M.cy, M.cz}, me[3] = {M.ex, M.ey, M.ez};
+                        for (int d = 0; d < 3; d++) {
+                            const float rc = mc[d] - c3[d];
+                            // rounding of the float centres and of the staged
+                            // coordinates: widen by 2^-20 of the magnitudes
+                            const float e = me[d] + 9.5367e-7f * (fabsf(mc[d]) + fabsf(c3[d]) + me[d]);
+                            B.lo[d] = fminf(B.lo[d], rc - e);
+                            B.hi[d] = fmaxf(B.hi[d], rc + e);
+                        }
+                        B.h2max = fmaxf(B.h2max, M.h2max);
+                    }
+                    s_box[s] = B;
+                }
+                __syncwarp();
+                mbar_arrive(&bar_full[s]);
             }
-            __syncthreads();
-
-            if (warp_rows) {
-                const TileBox B = *s_box;
-                bool far = B.empty;
-                if (!far) {
-                    float d2 = 0.f;
-#pragma unroll
-                    for (int d = 0; d < 3; d++) {
-                        const float slack = 9.5367e-7f * (fmaxf(fabsf(wlo[d]), fabsf(whi[d])));
-                        float gap = fmaxf(B.lo[d] - whi[d], wlo[d] - B.hi[d]) - slack;
-                        gap = fmaxf(gap, 0.f);
-                        d2 = fmaf(gap, gap, d2);
-                    }
-                    far = d2 > fmaxf(wh2, B.h2max) * 1.0001f;
-                }
-                // tile sums: acceleration two-level (sub-block -> tile), potential one level
-                f2 tx[K], ty[K], tz[K], pp[K];
-#pragma unroll
-                for (int k = 0; k < K; k++) tx[k] = ty[k] = tz[k] = pp[k] = pk(0.f, 0.f);
-
-                if (far) {
-                    for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
-                        f2 ax[K], ay[K], az[K];
-#pragma unroll
-                        for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pk(0.f, 0.f);
-#pragma unroll
-                        for (int s = 0; s < SUBQ; s++) {
-                            const int qd = base + s * Q;
-                            const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
-                            const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
-                            const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
-                            const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
-#pragma unroll
-                            for (int k = 0; k < K; k++) {
-                                f2 dx, dy, dz, r2;
-                                geom2(X.x, Y.x, Z.x, xi[k], yi[k], zi[k], dx, dy, dz, r2);
-                                accum2<NEWTON>(dx, dy, dz, r2, M.x, ax[k], ay[k], az[k], pp[k]);
-                                geom2(X.y, Y.y, Z.y, xi[k], yi[k], zi[k], dx, dy, dz, r2);
-                                accum2<NEWTON>(dx, dy, dz, r2, M.y, ax[k], ay[k], az[k], pp[k]);
-                            }
-                        }
-#pragma unroll
-                        for (int k = 0; k < K; k++) {
-                            tx[k] = add2(tx[k], ax[k]);
-                            ty[k] = add2(ty[k], ay[k]);
-                            tz[k] = add2(tz[k], az[k]);
-                        }
-                    }
-                } else {
-                    for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
-                        f2 ax[K], ay[K], az[K];
-#pragma unroll
-                        for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pk(0.f, 0.f);
-                        for (int s = 0; s < SUBQ; s++) {
-                            const int qd = base + s * Q;
-                            const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
-                            const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
-                            const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
-                            const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
-                            const float4 H = *reinterpret_cast<const float4 *>(&s_h[4 * qd]);
-#pragma unroll
-                            for (int k = 0; k < K; k++) {
-#pragma unroll
-                                for (int h = 0; h < 2; h++) {
-                                    f2 dx, dy, dz, r2;
-                                    geom2(h ? X.y : X.x, h ? Y.y : Y.x, h ? Z.y : Z.x, xi[k], yi[k],
-                                          zi[k], dx, dy, dz, r2);
-                                    f2 mj = h ? M.y : M.x;
-                                    float ra, rb;
-                                    upk(r2, ra, rb);
-                                    const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
-                                    const bool na = ra < fmaxf(h2i[k], ha);
-                                    const bool nb = rb < fmaxf(h2i[k], hb);
-                                    if (na || nb) {
-                                        const int jp0 = S.poff + jt + 4 * qd + 2 * h;
-                                        float *acc = s_acc + (k * 8) * NT + tid;
-                                        if (act[k] && na) near_fold<NEWTON>(D, a.nkernel, ip[k], jp0, acc, NT);
-                                        if (act[k] && nb) near_fold<NEWTON>(D, a.nkernel, ip[k], jp0 + 1, acc, NT);
-                                        float ma, mb;
-                                        upk(mj, ma, mb);
-                                        mj = pk(na ? 0.f : ma, nb ? 0.f : mb);
-                                        r2 = pk(na ? 1.f : ra, nb ? 1.f : rb);
-                                    }
-                                    accum2<NEWTON>(dx, dy, dz, r2, mj, ax[k], ay[k], az[k], pp[k]);
-                                }
-                            }
-                        }
-#pragma unroll
-                        for (int k = 0; k < K; k++) {
-                            tx[k] = add2(tx[k], ax[k]);
-                            ty[k] = add2(ty[k], ay[k]);
-                            tz[k] = add2(tz[k], az[k]);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    float *acc = s_acc + (k * 8) * NT + tid;
-                    fold(acc, acc + 4 * NT, tx[k]);
-                    fold(acc + NT, acc + 5 * NT, ty[k]);
-                    fold(acc + 2 * NT, acc + 6 * NT, tz[k]);
-                    fold(acc + 3 * NT, acc + 7 * NT, pp[k]);
-                }
-            }
-            __syncthreads();
-        }
-        if (failed) break;
-
-        // combine the Q threads of a row (fixed order), convert, write FP64 partials
-        double *p = a.partials + (size_t)(S.slot_off + W.tile * S.nchunks + W.chunk) * 4 * ITILE;
-        if (phase == 0) {
+        } else {
+            // ----------------------------------------------- consumer warps
+            int ip[K];
+            bool act[K];
+            f2 xi[K], yi[K], zi[K];
+            float h2i[K];
+            float wlo[3] = {INFINITY, INFINITY, INFINITY};
+            float whi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            float wh2 = 0.f;
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                if (!act[k]) continue;
                 const int li = warp * RPW * K + k * RPW + grp;
+                const int r = Wk.tile * ITILE + li;
+                act[k] = r < S.ni;
+                ip[k] = act[k] ? a.ilist[S.ioff + r] : 0;
+                float x = 1.0e15f, y = 1.0e15f, z = -1.0e15f, h2 = 0.f;
+                if (act[k]) {
+                    const int sl = ip[k];
+                    x = __fadd_rn(__fsub_rn(F.xh[sl], C.chx), __fsub_rn(F.xl[sl], C.clx));
+                    y = __fadd_rn(__fsub_rn(F.yh[sl], C.chy), __fsub_rn(F.yl[sl], C.cly));
+                    z = __fadd_rn(__fsub_rn(F.zh[sl], C.chz), __fsub_rn(F.zl[sl], C.clz));
+                    h2 = F.h2[sl];
+                    wlo[0] = fminf(wlo[0], x); whi[0] = fmaxf(whi[0], x);
+                    wlo[1] = fminf(wlo[1], y); whi[1] = fmaxf(whi[1], y);
+                    wlo[2] = fminf(wlo[2], z); whi[2] = fmaxf(whi[2], z);
+                    wh2 = fmaxf(wh2, h2);
+                }
+                xi[k] = pk(x, x);
+                yi[k] = pk(y, y);
+                zi[k] = pk(z, z);
+                h2i[k] = h2;
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    float h = s_acc[(k * 8 + c) * NT + tid], l = s_acc[(k * 8 + 4 + c) * NT + tid];
-                    for (int ph = 1; ph < Q; ph++) {
-                        ff_add(h, l, s_acc[(k * 8 + c) * NT + tid + ph]);
-                        l = __fadd_rn(l, s_acc[(k * 8 + 4 + c) * NT + tid + ph]);
+                for (int c = 0; c < 8; c++) s_acc[(k * 8 + c) * NT + tid] = 0.f;
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                for (int o = 16; o > 0; o >>= 1) {
+                    wlo[d] = fminf(wlo[d], __shfl_xor_sync(0xffffffffu, wlo[d], o));
+                    whi[d] = fmaxf(whi[d], __shfl_xor_sync(0xffffffffu, whi[d], o));
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) wh2 = fmaxf(wh2, __shfl_xor_sync(0xffffffffu, wh2, o));
+            const bool warp_rows = wlo[0] <= whi[0];
+            wh2 = wh2 * 1.00001f;
+            float slack[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) slack[d] = 9.5367e-7f * fmaxf(fabsf(wlo[d]), fabsf(whi[d]));
+
+            for (int t = 0; t < ntile; t++) {
+                const uint32_t gt = g + t;
+                const int s = gt % NS;
+                const bool ok = mbar_wait_bounded(&bar_full[s], (gt / NS) & 1, WAIT_LIMIT);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(a.err, DEVERR_TIMEOUT);
+                    failed = true;
+                    break;
+                }
+                const float *s_x = comp + s * 5 * TJ;
+                const float *s_y = s_x + TJ, *s_z = s_y + TJ, *s_m = s_z + TJ, *s_h = s_m + TJ;
+                const int jt = Wk.jb + t * TJ;
+                if (warp_rows) {
+                    const TileBox B = s_box[s];
+                    bool far = B.empty;
+                    if (!far) {
+                        float d2 = 0.f;
+#pragma unroll
+                        for (int d = 0; d < 3; d++) {
+                            float gap = fmaxf(B.lo[d] - whi[d], wlo[d] - B.hi[d]) - slack[d];
+                            gap = fmaxf(gap, 0.f);
+                            d2 = fmaf(gap, gap, d2);
+                        }
+                        far = d2 > fmaxf(wh2, B.h2max) * 1.0001f;
                     }
-                    const double v = ((double)h + (double)l) * (double)(c < 3 ? SA : SP);
-                    p[c * ITILE + li] = v;
+                    // tile sums: two levels (8-source sub-blocks -> tile)
+                    f2 tx[K], ty[K], tz[K], tp[K];
+#pragma unroll
+                    for (int k = 0; k < K; k++) tx[k] = ty[k] = tz[k] = tp[k] = pk(0.f, 0.f);
+
+                    if (far) {
+                        for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
+                            f2 ax[K], ay[K], az[K], pp[K];
+#pragma unroll
+                            for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
+#pragma unroll 2
+                            for (int u = 0; u < SUBQ; u++) {
+                                const int qd = base + u * Q;
+                                const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
+                                const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
+                                const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
+                                const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
+#pragma unroll
+                                for (int k = 0; k < K; k++) {
+                                    f2 dx, dy, dz, r2;
+                                    geom2(X.x, Y.x, Z.x, xi[k], yi[k], zi[k], dx, dy, dz, r2);
+                                    accum2<NEWTON>(dx, dy, dz, r2, M.x, ax[k], ay[k], az[k], pp[k]);
+                                    geom2(X.y, Y.y, Z.y, xi[k], yi[k], zi[k], dx, dy, dz, r2);
+                                    accum2<NEWTON>(dx, dy, dz, r2, M.y, ax[k], ay[k], az[k], pp[k]);
+                                }
+                            }
+#pragma unroll
+                            for (int k = 0; k < K; k++) {
+                                tx[k] = add2(tx[k], ax[k]);
+                                ty[k] = add2(ty[k], ay[k]);
+                                tz[k] = add2(tz[k], az[k]);
+                                tp[k] = add2(tp[k], pp[k]);
+                            }
+                        }
+                    } else {
+                        for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
+                            f2 ax[K], ay[K], az[K], pp[K];
+#pragma unroll
+                            for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
+                            for (int u = 0; u < SUBQ; u++) {
+                                const int qd = base + u * Q;
+                                const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
+                                const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
+                                const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
+                                const ulonglong2 M = *reinterpret_cast<const ulonglong2 *>(&s_m[4 * qd]);
+                                const float4 H = *reinterpret_cast<const float4 *>(&s_h[4 * qd]);
+#pragma unroll
+                                for (int k = 0; k < K; k++) {
+#pragma unroll
+                                    for (int h = 0; h < 2; h++) {
+                                        f2 dx, dy, dz, r2;
+                                        geom2(h ? X.y : X.x, h ? Y.y : Y.x, h ? Z.y : Z.x, xi[k],
+                                              yi[k], zi[k], dx, dy, dz, r2);
+                                        f2 mj = h ? M.y : M.x;
+                                        float ra, rb;
+                                        upk(r2, ra, rb);
+                                        const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
+                                        const bool na = ra < fmaxf(h2i[k], ha);
+                                        const bool nb = rb < fmaxf(h2i[k], hb);
+                                        if (na || nb) {
+                                            const int jp0 = S.poff + jt + 4 * qd + 2 * h;
+                                            float *acc = s_acc + (k * 8) * NT + tid;
+                                            if (act[k] && na)
+                                                near_fold<NEWTON>(D, a.nkernel, ip[k], jp0, acc, NT);
+                                            if (act[k] && nb)
+                                                near_fold<NEWTON>(D, a.nkernel, ip[k], jp0 + 1, acc, NT);
+                                            float ma, mb;
+                                            upk(mj, ma, mb);
+                                            mj = pk(na ? 0.f : ma, nb ? 0.f : mb);
+                                            r2 = pk(na ? 1.f : ra, nb ? 1.f : rb);
+                                        }
+                                        accum2<NEWTON>(dx, dy, dz, r2, mj, ax[k], ay[k], az[k], pp[k]);
+                                    }
+                                }
+                            }
+#pragma unroll
+                            for (int k = 0; k < K; k++) {
+                                tx[k] = add2(tx[k], ax[k]);
+                                ty[k] = add2(ty[k], ay[k]);
+                                tz[k] = add2(tz[k], az[k]);
+                                tp[k] = add2(tp[k], pp[k]);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        float *acc = s_acc + (k * 8) * NT + tid;
+                        fold(acc, acc + 4 * NT, tx[k]);
+                        fold(acc + NT, acc + 5 * NT, ty[k]);
+                        fold(acc + 2 * NT, acc + 6 * NT, tz[k]);
+                        fold(acc + 3 * NT, acc + 7 * NT, tp[k]);
+                    }
+                }
+                mbar_arrive(&bar_empty[s]);
+            }
+            if (!failed) {
+                // combine the Q threads of a row (fixed order), convert, write FP64 partials
+                __syncwarp();
+                double *p = a.partials +
+                            (size_t)(S.slot_off + Wk.tile * S.nchunks + Wk.chunk) * 4 * ITILE;
+                if (phase == 0) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        if (!act[k]) continue;
+                        const int li = warp * RPW * K + k * RPW + grp;
+#pragma unroll
+                        for (int c = 0; c < 4; c++) {
+                            float h = s_acc[(k * 8 + c) * NT + tid];
+                            float l = s_acc[(k * 8 + 4 + c) * NT + tid];
+                            for (int ph = 1; ph < Q; ph++) {
+                                ff_add(h, l, s_acc[(k * 8 + c) * NT + tid + ph]);
+                                l = __fadd_rn(l, s_acc[(k * 8 + 4 + c) * NT + tid + ph]);
+                            }
+                            p[c * ITILE + li] = ((double)h + (double)l) * (double)(c < 3 ? SA : SP);
+                        }
+                    }
                 }
             }
         }
-        __syncthreads();
+        g += ntile;
     }
-    // never leave with bulk copies in flight into this CTA's shared memory:
-    // a copy is outstanding iff a buffer was issued and not yet waited for
-    if (failed && tid == 0) {
+    // never leave with bulk copies in flight into this CTA's shared memory
+    if (producer && lane == 0) {
         for (int b = 0; b < 2; b++)
-            if (pending[b]) mbar_wait_bounded(&bar[b], uses[b] & 1, WAIT_LIMIT);
+            if (pending[b]) mbar_wait_bounded(&bar_raw[b], pend_par[b], WAIT_LIMIT);
     }
 }
 
-#define SG_F32_VARIANTS(X)                                   \
-    X(256, 4, 1, 256, true, "f32split_nt256_k4_q1_tj256")     \
-    X(256, 2, 1, 256, true, "f32split_nt256_k2_q1_tj256")     \
-    X(128, 4, 1, 256, true, "f32split_nt128_k4_q1_tj256")     \
-    X(128, 2, 1, 256, true, "f32split_nt128_k2_q1_tj256")     \
-    X(256, 2, 2, 256, true, "f32split_nt256_k2_q2_tj256")     \
-    X(256, 1, 4, 256, true, "f32split_nt256_k1_q4_tj256")     \
-    X(256, 4, 1, 256, false, "f32split_nt256_k4_q1_tj256_nonewton")
+// name, consumer warps W, rows per thread K, threads per row Q, j-tile TJ, stages NS, Newton step
+#define SG_F32_VARIANTS(X)                                         \
+    X(8, 2, 1, 256, 4, true, "f32split_w8_k2_q1_tj256")             \
+    X(11, 2, 1, 256, 4, true, "f32split_w11_k2_q1_tj256")           \
+    X(15, 1, 1, 256, 4, true, "f32split_w15_k1_q1_tj256")           \
+    X(8, 1, 2, 256, 4, true, "f32split_w8_k1_q2_tj256")             \
+    X(8, 1, 4, 256, 4, true, "f32split_w8_k1_q4_tj256")             \
+    X(8, 2, 1, 256, 4, false, "f32split_w8_k2_q1_tj256_nonewton")
 
-#define SG_INFO(NT, K, Q, TJ, NW, NAME) {1, NT, K, Q, TJ, NW ? 1 : 0, NAME},
+#define SG_INFO(W, K, Q, TJ, NS, NW, NAME) {1, (W + 1) * 32, K, Q, TJ, NW ? 1 : 0, NAME, W * 32 * K / Q},
 static const VariantInfo kF32Variants[] = {SG_F32_VARIANTS(SG_INFO)};
 #undef SG_INFO
-#define SG_PTR(NT, K, Q, TJ, NW, NAME) (const void *)k_f32split<NT, K, Q, TJ, NW>,
+#define SG_PTR(W, K, Q, TJ, NS, NW, NAME) (const void *)k_f32split<W, K, Q, TJ, NS, NW>,
 static const void *kF32Kernels[] = {SG_F32_VARIANTS(SG_PTR)};
 #undef SG_PTR
-#define SG_SMEM(NT, K, Q, TJ, NW, NAME) F32Smem<NT, K, TJ>::BYTES,
+#define SG_SMEM(W, K, Q, TJ, NS, NW, NAME) WsSmem<W, K, TJ, NS>::BYTES,
 static const int kF32Smem[] = {SG_F32_VARIANTS(SG_SMEM)};
 #undef SG_SMEM
 constexpr int kNF32 = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
@@ -464,12 +511,12 @@ cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st)
     cudaError_t e = f32_prepare(v);
     if (e != cudaSuccess) return e;
     int idx = 0;
-#define SG_CASE(NT, K, Q, TJ, NW, NAME)                                                \
-    if (v == idx) {                                                                    \
-        k_f32split<NT, K, Q, TJ, NW><<<grid, NT, F32Smem<NT, K, TJ>::BYTES, st>>>(a);  \
-        ++g_launches;                                                                  \
-        return cudaGetLastError();                                                     \
-    }                                                                                  \
+#define SG_CASE(W, K, Q, TJ, NS, NW, NAME)                                                    \
+    if (v == idx) {                                                                           \
+        k_f32split<W, K, Q, TJ, NS, NW><<<grid, (W + 1) * 32, WsSmem<W, K, TJ, NS>::BYTES, st>>>(a); \
+        ++g_launches;                                                                         \
+        return cudaGetLastError();                                                            \
+    }                                                                                         \
     ++idx;
     SG_F32_VARIANTS(SG_CASE)
 #undef SG_CASE

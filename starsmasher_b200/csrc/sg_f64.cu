@@ -116,9 +116,9 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
 }
 
 static const VariantInfo kF64Variants[] = {
-    {0, 128, 1, 1, 128, 0, "fp64_nt128_k1_tj128"},
-    {0, 256, 1, 1, 256, 0, "fp64_nt256_k1_tj256"},
-    {0, 128, 2, 1, 128, 0, "fp64_nt128_k2_tj128"},
+    {0, 128, 1, 1, 128, 0, "fp64_nt128_k1_tj128", 128},
+    {0, 256, 1, 1, 256, 0, "fp64_nt256_k1_tj256", 256},
+    {0, 128, 2, 1, 128, 0, "fp64_nt128_k2_tj128", 256},
 };
 static const void *kF64Kernels[] = {
     (const void *)k_fp64<128, 1, 128>,

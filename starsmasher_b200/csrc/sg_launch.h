@@ -69,7 +69,8 @@ struct VariantInfo {
     int tj;         // j-tile
     int newton;     // one Newton step on rsqrt (f32 only)
     const char *name;
-    int itile() const { return nt * k / q; }
+    int rows;       // rows per i-tile
+    int itile() const { return rows; }
 };
 int variant_count(int precision);
 const VariantInfo &variant_info(int precision, int v);
