@@ -319,6 +319,20 @@ static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     const int occ = variant_occupancy(precision, variant);
     const int resident = occ * c->sm_count;
     const int target = 4 * resident;
+    // One set: items are all alike, so pick the chunk count whose item count
+    // fills the last wave of persistent CTAs best (ties: fewer chunks).
+    int single_nch = 0;
+    if (P.nsets == 1 && P.ntiles > 0) {
+        const SetDesc &d = P.sets[0];
+        const int jtiles = (d.n + P.tj - 1) / P.tj;
+        const int maxch = std::max(1, std::min(jtiles, std::min(64, (int)(((long long)jtiles * P.tj) / kMinChunkJ))));
+        double best = -1.0;
+        for (int nch = 1; nch <= maxch; nch++) {
+            const double waves = (double)P.ntiles * nch / resident;
+            const double eff = waves / std::ceil(waves) - 0.002 * nch;  // small per-chunk cost
+            if (eff > best + 1e-9) { best = eff; single_nch = nch; }
+        }
+    }
     int slot = 0;
     P.nchunks_max = 1;
     struct Cost { long long cost; WorkItem w; };
@@ -329,6 +343,7 @@ static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
         int nch = P.ntiles > 0 ? (target + P.ntiles - 1) / P.ntiles : 1;
         const int maxch = std::max(1, (int)(((long long)jtiles * P.tj) / kMinChunkJ));
         nch = std::max(1, std::min(nch, std::min(maxch, std::max(1, jtiles))));
+        if (single_nch > 0) nch = single_nch;
         d.nchunks = nch;
         d.slot_off = slot;
         slot += d.ntiles * nch;

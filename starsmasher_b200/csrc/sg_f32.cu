@@ -132,7 +132,9 @@ struct WsSmem {
     static constexpr int COMP = META + 2 * NMETA * 32;     // [NS][5][TJ] floats
     static constexpr int BOX = COMP + NS * 5 * TJ * 4;     // [NS] TileBox
     static constexpr int ACC = BOX + NS * 32;              // [K*8][NT] floats
-    static constexpr int BAR = ACC + K * 8 * NT * 4;       // 2 + 2*NS mbarriers
+    static constexpr int NEARCAP = 16;                     // deferred near pairs per thread
+    static constexpr int NEAR = ACC + K * 8 * NT * 4;      // [NEARCAP][NT] ushort
+    static constexpr int BAR = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // 2 + 2*NS mbarriers
     static constexpr int ITEM = BAR + (2 + 2 * NS) * 8;    // 2 ints
     static constexpr int BYTES = ITEM + 16;
     static constexpr uint32_t TX = 8 * TJ * 4 + NMETA * 32;  // bytes per tile
@@ -152,6 +154,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     constexpr int NMETA = L::NMETA;
     constexpr float SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
     constexpr uint32_t WAIT_LIMIT = 1u << 22;
+    constexpr int NOVF = TJ / 4;           // "no overflow" marker of the near list
+    constexpr int NEARCAP = L::NEARCAP;
 
     extern __shared__ __align__(128) unsigned char smem[];
     float *raw = reinterpret_cast<float *>(smem + L::RAW);
@@ -159,6 +163,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     float *comp = reinterpret_cast<float *>(smem + L::COMP);
     TileBox *s_box = reinterpret_cast<TileBox *>(smem + L::BOX);
     float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
+    unsigned short *s_near = reinterpret_cast<unsigned short *>(smem + L::NEAR);
     uint64_t *bar_raw = reinterpret_cast<uint64_t *>(smem + L::BAR);  // [2]
     uint64_t *bar_full = bar_raw + 2;                                  // [NS]
     uint64_t *bar_empty = bar_full + NS;                               // [NS]
@@ -345,6 +350,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     f2 tx[K], ty[K], tz[K], tp[K];
 #pragma unroll
                     for (int k = 0; k < K; k++) tx[k] = ty[k] = tz[k] = tp[k] = pk(0.f, 0.f);
+                    int nlist = 0, ovf = NOVF;
 
                     if (far) {
                         for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
@@ -376,12 +382,15 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                             }
                         }
                     } else {
+                        // near pairs are masked here and recorded (row k, source j)
+                        // in this thread's list; FP64 evaluation runs after the loop
                         for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
                             f2 ax[K], ay[K], az[K], pp[K];
 #pragma unroll
                             for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
                             for (int u = 0; u < SUBQ; u++) {
                                 const int qd = base + u * Q;
+                                const int n0 = nlist;
                                 const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
                                 const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
                                 const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
@@ -401,12 +410,20 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                                         const bool na = ra < fmaxf(h2i[k], ha);
                                         const bool nb = rb < fmaxf(h2i[k], hb);
                                         if (na || nb) {
-                                            const int jp0 = S.poff + jt + 4 * qd + 2 * h;
-                                            float *acc = s_acc + (k * 8) * NT + tid;
-                                            if (act[k] && na)
-                                                near_fold<NEWTON>(D, a.nkernel, ip[k], jp0, acc, NT);
-                                            if (act[k] && nb)
-                                                near_fold<NEWTON>(D, a.nkernel, ip[k], jp0 + 1, acc, NT);
+                                            if (ovf == NOVF && act[k]) {
+                                                const int j0 = 4 * qd + 2 * h;
+                                                if (na) {
+                                                    if (nlist < NEARCAP) s_near[nlist * NT + tid] = (k << 8) | j0;
+                                                    else ovf = qd;
+                                                    nlist++;
+                                                }
+                                                if (nb) {
+                                                    if (nlist < NEARCAP) s_near[nlist * NT + tid] = (k << 8) | (j0 + 1);
+                                                    else ovf = qd;
+                                                    nlist++;
+                                                }
+                                                if (ovf != NOVF) nlist = n0;  // the rescan redoes this quad
+                                            }
                                             float ma, mb;
                                             upk(mj, ma, mb);
                                             mj = pk(na ? 0.f : ma, nb ? 0.f : mb);
@@ -432,6 +449,45 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                         fold(acc + NT, acc + 5 * NT, ty[k]);
                         fold(acc + 2 * NT, acc + 6 * NT, tz[k]);
                         fold(acc + 3 * NT, acc + 7 * NT, tp[k]);
+                    }
+                    if (!far) {
+                        // deferred near-field pairs in FP64, in the order found
+                        for (int e = 0; e < nlist; e++) {
+                            const int v = s_near[e * NT + tid];
+                            const int kk = v >> 8, j = v & 255;
+                            int ipk = ip[0];
+#pragma unroll
+                            for (int k = 1; k < K; k++)
+                                if (kk == k) ipk = ip[k];
+                            near_fold<NEWTON>(D, a.nkernel, ipk, S.poff + jt + j,
+                                              s_acc + (kk * 8) * NT + tid, NT);
+                        }
+                        // list overflow: rescan this thread's quads from the overflow
+                        // point with the same float test and evaluate every near pair
+                        for (int qd = ovf; qd < TJ / 4; qd += Q) {
+                            const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
+                            const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
+                            const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
+                            const float4 H = *reinterpret_cast<const float4 *>(&s_h[4 * qd]);
+#pragma unroll
+                            for (int k = 0; k < K; k++) {
+                                if (!act[k]) continue;
+#pragma unroll
+                                for (int h = 0; h < 2; h++) {
+                                    f2 dx, dy, dz, r2;
+                                    geom2(h ? X.y : X.x, h ? Y.y : Y.x, h ? Z.y : Z.x, xi[k], yi[k],
+                                          zi[k], dx, dy, dz, r2);
+                                    float ra, rb;
+                                    upk(r2, ra, rb);
+                                    const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
+                                    const int jp0 = S.poff + jt + 4 * qd + 2 * h;
+                                    if (ra < fmaxf(h2i[k], ha))
+                                        near_fold<NEWTON>(D, a.nkernel, ip[k], jp0, s_acc + (k * 8) * NT + tid, NT);
+                                    if (rb < fmaxf(h2i[k], hb))
+                                        near_fold<NEWTON>(D, a.nkernel, ip[k], jp0 + 1, s_acc + (k * 8) * NT + tid, NT);
+                                }
+                            }
+                        }
                     }
                 }
                 mbar_arrive(&bar_empty[s]);
@@ -471,12 +527,12 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 
 // name, consumer warps W, rows per thread K, threads per row Q, j-tile TJ, stages NS, Newton step
 #define SG_F32_VARIANTS(X)                                         \
+    X(15, 2, 1, 256, 4, true, "f32split_w15_k2_q1_tj256")           \
     X(8, 2, 1, 256, 4, true, "f32split_w8_k2_q1_tj256")             \
-    X(11, 2, 1, 256, 4, true, "f32split_w11_k2_q1_tj256")           \
     X(15, 1, 1, 256, 4, true, "f32split_w15_k1_q1_tj256")           \
-    X(8, 1, 2, 256, 4, true, "f32split_w8_k1_q2_tj256")             \
+    X(15, 1, 2, 256, 4, true, "f32split_w15_k1_q2_tj256")           \
     X(8, 1, 4, 256, 4, true, "f32split_w8_k1_q4_tj256")             \
-    X(8, 2, 1, 256, 4, false, "f32split_w8_k2_q1_tj256_nonewton")
+    X(15, 2, 1, 256, 4, false, "f32split_w15_k2_q1_tj256_nonewton")
 
 #define SG_INFO(W, K, Q, TJ, NS, NW, NAME) {1, (W + 1) * 32, K, Q, TJ, NW ? 1 : 0, NAME, W * 32 * K / Q},
 static const VariantInfo kF32Variants[] = {SG_F32_VARIANTS(SG_INFO)};
