@@ -55,6 +55,11 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--variant", type=int, default=-1,
                    help="force a kernel variant of --precision (default: tuned/automatic)")
+    p.add_argument("--graph", action="store_true",
+                   help="batched workloads: each step replays a captured CUDA graph of "
+                        "(seeded 1e-3 position kick + gravity) on device-resident state")
+    p.add_argument("--no-separate", action="store_true",
+                   help="batched workloads: skip the one-call-per-set comparison")
     return p.parse_args()
 
 
@@ -249,19 +254,39 @@ def main():
     outs = [torch.empty(n, dtype=dt, device=f"cuda:{device}") for _ in range(4)]
     W = torch.empty(ws.nsets, dtype=dt, device=f"cuda:{device}")
 
-    def step(precision):
+    def gravity(precision):
         if batched:
             ctx.batch_forces_device(ws.offsets, *X, *outs, W=W, nkernel=args.nkernel,
                                     precision=precision)
         else:
             ctx.forces_device(n, *X, *outs, W=W, nkernel=args.nkernel, precision=precision)
 
+    graph = None
+    sigma, kick_seed = 1e-3, 12345
+
+    def step(precision):
+        if graph is not None and precision == args.precision:
+            graph.launch(1)
+        else:
+            gravity(precision)
+
     # L2 flush buffer (> 126 MB L2), written between timed steps
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")
 
     for _ in range(max(3, args.warmup)):
-        step(args.precision)
+        gravity(args.precision)
     torch.cuda.synchronize()
+    if args.graph:
+        # device-resident sweep: every replay kicks the positions (seeded,
+        # sigma = 1e-3 R) and recomputes gravity, all inside one CUDA graph
+        ctx.kick_reset(0)
+        with ctx.capture() as cap:
+            ctx.kick_device(n, X[0], X[1], X[2], sigma, kick_seed)
+            gravity(args.precision)
+        graph = cap.graph
+        for _ in range(max(3, args.warmup)):
+            graph.launch(1)
+        torch.cuda.synchronize()
 
     def barrier():
         if world > 1:
@@ -298,6 +323,35 @@ def main():
     ms_per_step = total_ms / args.steps
     value = pairs * world * args.steps / (total_ms * 1e-3) / 1e9
     res_f32 = [o.cpu().numpy() for o in outs]
+    graph_info = None
+    if graph is not None:
+        graph_info = {"calls_timed": args.steps, "ms_per_call": ms_per_step,
+                      "kick_sigma": sigma, "nodes": "kick + sort/gather/tiles + pair kernel + merge"}
+        graph.close()
+        graph = None
+
+    # ------------------------------------- batched vs one call per set
+    batch_cmp = None
+    if batched and not args.no_separate:
+        def separate():
+            for s in range(ws.nsets):
+                a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
+                ctx.forces_device(b - a, *(t[a:b] for t in X), *(o[a:b] for o in outs),
+                                  nkernel=args.nkernel, precision=args.precision)
+        separate()
+        torch.cuda.synchronize()
+        reps = max(1, min(args.steps, 3))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            separate()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sep_ms = e0.elapsed_time(e1) / reps
+        batch_cmp = {"separate_calls_ms_per_step": sep_ms, "batched_ms_per_step": ms_per_step,
+                     "speedup_batched_vs_separate": sep_ms / ms_per_step,
+                     "separate": f"{ws.nsets} sphgrav_forces_device calls, one per set"}
 
     # --------------------------------------------- FP64 kernel and accuracy
     fp64 = None
@@ -396,6 +450,10 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "fp64": fp64, "accuracy_vs_fp64": acc,
         }
+        if batch_cmp:
+            line["batch_vs_separate"] = batch_cmp
+        if graph_info:
+            line["graph_sweep"] = graph_info
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

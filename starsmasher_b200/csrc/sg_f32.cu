@@ -32,12 +32,13 @@
 //   * sums run in FP32 over sub-blocks of 8 sources per lane, are added into
 //     a per-tile FP32 sum that folds into compensated (TwoSum, "Kahan") float
 //     hi/lo accumulators in shared memory once per tile.
-//   * pairs with r^2 < max(H_i^2, H_j^2) -- the softened near field, where
-//     the reference polynomials cancel by up to ~1e3 near q = 1 -- are
-//     evaluated in FP64 (pair_f64_slots, the CPU-path formulas) and folded
-//     into the same accumulators.  A warp skips the per-pair near test for
-//     a tile when the bounding boxes of its rows and of the tile are farther
-//     apart than the largest H of both.
+//   * pairs with r < 2 max(H_i, H_j) are evaluated in FP64 (pair_f64_slots,
+//     the CPU-path formulas) after the tile's FP32 loop and folded into the
+//     same accumulators: below H the softened near field, whose reference
+//     polynomials cancel by up to ~1e3 near q = 1, and between H and 2H the
+//     largest Newtonian terms (see FP64_BAND2).  A warp skips the per-pair
+//     test for a tile when the bounding boxes of its rows and of the tile are
+//     farther apart than 2 max(H) of both.
 //   * per (row, j-chunk) results leave the CTA as FP64 partial sums merged in
 //     chunk order (k_merge).
 // Reference kernel replaced: dev_compute_forces / dev_force_ij_nkernel*
@@ -122,6 +123,14 @@ __device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, i
     ff_add_d(acc[3 * stride], acc[7 * stride], o.pot / SP);
 }
 
+// Pairs with r^2 < FP64_BAND2 * max(H_i^2, H_j^2), i.e. r < 2 max(H), take the
+// FP64 path.  Below H that is the softened near field (reference polynomials,
+// which cancel in FP32); between H and 2H it is the Newtonian term in FP64:
+// these are the largest far-field terms, and in FP32 their rounding alone
+// sets a ~1e-6 floor on the relative error of a particle whose acceleration
+// cancels (|a| ~ 0.05 max), while they are only ~1e-3 of all pairs at N=1M.
+constexpr float FP64_BAND2 = 4.0f;
+
 // Shared-memory layout of one CTA (dynamic shared memory, byte offsets).
 template <int W, int K, int TJ, int NS>
 struct WsSmem {
@@ -132,7 +141,7 @@ struct WsSmem {
     static constexpr int COMP = META + 2 * NMETA * 32;     // [NS][5][TJ] floats
     static constexpr int BOX = COMP + NS * 5 * TJ * 4;     // [NS] TileBox
     static constexpr int ACC = BOX + NS * 32;              // [K*8][NT] floats
-    static constexpr int NEARCAP = 16;                     // deferred near pairs per thread
+    static constexpr int NEARCAP = 32;                     // deferred near pairs per thread
     static constexpr int NEAR = ACC + K * 8 * NT * 4;      // [NEARCAP][NT] ushort
     static constexpr int BAR = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // 2 + 2*NS mbarriers
     static constexpr int ITEM = BAR + (2 + 2 * NS) * 8;    // 2 ints
@@ -244,7 +253,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     cx[2 * TJ + j] = __fadd_rn(__fsub_rn(rbuf[4 * TJ + j], C.chz),
                                                __fsub_rn(rbuf[5 * TJ + j], C.clz));
                     cx[3 * TJ + j] = rbuf[6 * TJ + j];
-                    cx[4 * TJ + j] = rbuf[7 * TJ + j];
+                    cx[4 * TJ + j] = FP64_BAND2 * rbuf[7 * TJ + j];  // (2H)^2: exact scaling
                 }
                 if (lane == 0) {
                     TileBox B;
@@ -266,7 +275,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                             B.lo[d] = fminf(B.lo[d], rc - e);
                             B.hi[d] = fmaxf(B.hi[d], rc + e);
                         }
-                        B.h2max = fmaxf(B.h2max, M.h2max);
+                        B.h2max = fmaxf(B.h2max, FP64_BAND2 * M.h2max);
                     }
                     s_box[s] = B;
                 }
@@ -294,7 +303,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     x = __fadd_rn(__fsub_rn(F.xh[sl], C.chx), __fsub_rn(F.xl[sl], C.clx));
                     y = __fadd_rn(__fsub_rn(F.yh[sl], C.chy), __fsub_rn(F.yl[sl], C.cly));
                     z = __fadd_rn(__fsub_rn(F.zh[sl], C.chz), __fsub_rn(F.zl[sl], C.clz));
-                    h2 = F.h2[sl];
+                    h2 = FP64_BAND2 * F.h2[sl];
                     wlo[0] = fminf(wlo[0], x); whi[0] = fmaxf(whi[0], x);
                     wlo[1] = fminf(wlo[1], y); whi[1] = fmaxf(whi[1], y);
                     wlo[2] = fminf(wlo[2], z); whi[2] = fmaxf(whi[2], z);
