@@ -189,6 +189,26 @@ int sphgrav_force_variant(sphgrav_ctx *ctx, int precision, int variant);
 int sphgrav_variant_count(int precision);
 const char *sphgrav_variant_name(int precision, int variant);
 
+/* ----------------------------------------------- no device allocation ---
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (during a CUDA graph capture, under a host's own memory pool, or
+ * after start-up): FP64 forces of one set, all pointers DEVICE pointers of
+ * length n, every row computed, enqueued on `stream` (a cudaStream_t; NULL is
+ * the default stream).  Calls no cudaMalloc/cudaFree or allocating routine;
+ * its only scratch is a static device array of SPHGRAV_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading this library holds until the process exits, which
+ * caps n at SPHGRAV_NOALLOC_MAX_N (SPHGRAV_ERR_TOO_LARGE beyond).  The first
+ * call on a device looks up that array's device address; make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race.  Particle data
+ * are not validated (mass > 0 and range2 != 0 are the caller's contract). */
+#define SPHGRAV_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define SPHGRAV_NOALLOC_MAX_N 262144
+int sphgrav_forces_fp64_noalloc(int n, const double *x, const double *y, const double *z,
+                                const double *mass, const double *range2, int nkernel,
+                                double *ax, double *ay, double *az, double *pot,
+                                void *stream);
+
 /* ------------------------------------------------------- diagnostics --- */
 const char *sphgrav_status_string(int status);
 /* Last error message recorded on this thread (CUDA error text and context). */
