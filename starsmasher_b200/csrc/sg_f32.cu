@@ -111,12 +111,24 @@ __device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
 // Near-field pair (r^2 < max H^2) in FP64, folded into the row's
 // compensated accumulators acc[c * stride] (hi) / acc[(4 + c) * stride] (lo),
 // in the accumulators' scaled units.
-template <bool NEWTON>
-__device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, int jp, float *acc,
-                                       int stride)
+// The source's data come from the staged raw tile `rs` (index j): the hi + lo
+// position pair (a 48-bit representation of the FP64 position, exact in
+// double) and its FP64 mass and H^2; the row's position is rebuilt from its
+// own hi + lo pair so that coincident particles give dr == 0 exactly.
+template <bool NEWTON, int TJ>
+__device__ __noinline__ void near_fold(const SortedF64 D, const SortedF32 F, int nkernel, int ip,
+                                       int jp, const float *rs, int j, float *acc, int stride)
 {
     constexpr double SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
-    const PairOut o = pair_f64_slots(D, nkernel, ip, jp);
+    const double *rd = reinterpret_cast<const double *>(rs + 8 * TJ);
+    const double xi = (double)F.xh[ip] + (double)F.xl[ip];
+    const double yi = (double)F.yh[ip] + (double)F.yl[ip];
+    const double zi = (double)F.zh[ip] + (double)F.zl[ip];
+    const double xj = (double)rs[j] + (double)rs[TJ + j];
+    const double yj = (double)rs[2 * TJ + j] + (double)rs[3 * TJ + j];
+    const double zj = (double)rs[4 * TJ + j] + (double)rs[5 * TJ + j];
+    const PairOut o = pair_f64_core(D, nkernel, ip, jp, xj - xi, yj - yi, zj - zi, rd[j], D.h2[ip],
+                                    rd[TJ + j]);
     ff_add_d(acc[0], acc[4 * stride], o.ax / SA);
     ff_add_d(acc[stride], acc[5 * stride], o.ay / SA);
     ff_add_d(acc[2 * stride], acc[6 * stride], o.az / SA);
@@ -136,17 +148,20 @@ template <int W, int K, int TJ, int NS>
 struct WsSmem {
     static constexpr int NT = W * 32;
     static constexpr int NMETA = TJ / META_J;
-    static constexpr int RAW = 0;                          // [2][8][TJ] floats (TMA targets)
-    static constexpr int META = RAW + 2 * 8 * TJ * 4;      // [2][NMETA] JMeta (TMA targets)
-    static constexpr int COMP = META + 2 * NMETA * 32;     // [NS][5][TJ] floats
+    // raw stage (TMA target): 8 float arrays x_hi x_lo y_hi y_lo z_hi z_lo m H^2,
+    // then 2 double arrays m, H^2
+    static constexpr int RAWSTAGE = 8 * TJ * 4 + 2 * TJ * 8;
+    static constexpr int RAW = 0;                          // [NS] raw stages
+    static constexpr int META = RAW + NS * RAWSTAGE;       // [NS][NMETA] JMeta (TMA targets)
+    static constexpr int COMP = META + NS * NMETA * 32;    // [NS][5][TJ] floats
     static constexpr int BOX = COMP + NS * 5 * TJ * 4;     // [NS] TileBox
     static constexpr int ACC = BOX + NS * 32;              // [K*8][NT] floats
     static constexpr int NEARCAP = 32;                     // deferred near pairs per thread
     static constexpr int NEAR = ACC + K * 8 * NT * 4;      // [NEARCAP][NT] ushort
-    static constexpr int BAR = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // 2 + 2*NS mbarriers
-    static constexpr int ITEM = BAR + (2 + 2 * NS) * 8;    // 2 ints
+    static constexpr int BAR = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // 3*NS mbarriers
+    static constexpr int ITEM = BAR + 3 * NS * 8;          // 2 ints
     static constexpr int BYTES = ITEM + 16;
-    static constexpr uint32_t TX = 8 * TJ * 4 + NMETA * 32;  // bytes per tile
+    static constexpr uint32_t TX = RAWSTAGE + NMETA * 32;  // bytes per tile
 };
 
 template <int W, int K, int Q, int TJ, int NS, bool NEWTON>
@@ -167,14 +182,13 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     constexpr int NEARCAP = L::NEARCAP;
 
     extern __shared__ __align__(128) unsigned char smem[];
-    float *raw = reinterpret_cast<float *>(smem + L::RAW);
     JMeta *s_meta = reinterpret_cast<JMeta *>(smem + L::META);
     float *comp = reinterpret_cast<float *>(smem + L::COMP);
     TileBox *s_box = reinterpret_cast<TileBox *>(smem + L::BOX);
     float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
     unsigned short *s_near = reinterpret_cast<unsigned short *>(smem + L::NEAR);
-    uint64_t *bar_raw = reinterpret_cast<uint64_t *>(smem + L::BAR);  // [2]
-    uint64_t *bar_full = bar_raw + 2;                                  // [NS]
+    uint64_t *bar_raw = reinterpret_cast<uint64_t *>(smem + L::BAR);  // [NS]
+    uint64_t *bar_full = bar_raw + NS;                                 // [NS]
     uint64_t *bar_empty = bar_full + NS;                               // [NS]
     int *s_item = reinterpret_cast<int *>(smem + L::ITEM);             // [2]
 
@@ -186,9 +200,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     const SortedF32 F = a.F;
 
     if (tid == 0) {
-        mbar_init(&bar_raw[0], 1);
-        mbar_init(&bar_raw[1], 1);
         for (int s = 0; s < NS; s++) {
+            mbar_init(&bar_raw[s], 1);     // TMA transaction count
             mbar_init(&bar_full[s], 32);   // every producer lane arrives
             mbar_init(&bar_empty[s], NT);  // every consumer thread arrives
         }
@@ -198,22 +211,31 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 
     uint32_t g = 0;                        // tiles this CTA has passed through its ring
     bool failed = false;
-    bool pending[2] = {false, false};      // producer lane 0: raw copies in flight
-    uint32_t pend_par[2] = {0u, 0u};       // ... and the barrier phase they complete
+    bool pending[NS];                      // producer lane 0: raw copies in flight per stage
+    uint32_t pend_par[NS];                 // ... and the barrier phase they complete
+#pragma unroll
+    for (int s = 0; s < NS; s++) { pending[s] = false; pend_par[s] = 0u; }
 
-    // bulk copies of set-local slots [jt, jt+TJ) (ring tile gt) into raw buffer gt & 1
+    // bulk copies of set-local slots [jt, jt+TJ) (ring tile gt) into raw stage gt % NS;
+    // the caller has seen that stage's consumers release it
     auto issue = [&](const SetDesc &S, int jt, uint32_t gt) {
-        const int b = gt & 1;
-        float *dst = raw + b * 8 * TJ;
+        const int b = gt % NS;
+        float *dst = reinterpret_cast<float *>(smem + L::RAW + b * L::RAWSTAGE);
+        double *dstd = reinterpret_cast<double *>(dst + 8 * TJ);
         const int s0 = S.poff + jt;
         pending[b] = true;
-        pend_par[b] = (gt >> 1) & 1;
-        fence_mbar_init();  // order earlier generic reads of the buffer before the async writes
+        pend_par[b] = (gt / NS) & 1;
+        fence_mbar_init();  // order earlier generic reads of the stage before the async writes
         mbar_arrive_expect_tx(&bar_raw[b], L::TX);
         const float *src[8] = {F.xh, F.xl, F.yh, F.yl, F.zh, F.zl, F.m, F.h2};
 #pragma unroll
         for (int k = 0; k < 8; k++) bulk_g2s(dst + k * TJ, src[k] + s0, TJ * 4, &bar_raw[b]);
+        bulk_g2s(dstd, D.m + s0, TJ * 8, &bar_raw[b]);
+        bulk_g2s(dstd + TJ, D.h2 + s0, TJ * 8, &bar_raw[b]);
         bulk_g2s(s_meta + b * NMETA, a.jmeta + S.meta_off + jt / META_J, NMETA * 32, &bar_raw[b]);
+    };
+    auto stage_raw = [&](int s) -> const float * {
+        return reinterpret_cast<const float *>(smem + L::RAW + s * L::RAWSTAGE);
     };
 
     for (int iter = 0;; iter++) {
@@ -228,22 +250,36 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 
         if (producer) {
             // ------------------------------------------------ producer warp
-            if (lane == 0 && ntile > 0) issue(S, Wk.jb, g);
+            // A stage (raw tile + computed tile) is reused for ring tile gt once the
+            // consumers released tile gt - NS: wait for that before each bulk copy.
+            if (ntile > 0) {
+                const bool ok = mbar_wait_bounded(&bar_empty[g % NS], ((g / NS) & 1) ^ 1, WAIT_LIMIT);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(a.err, DEVERR_TIMEOUT);
+                    failed = true;
+                } else if (lane == 0) {
+                    issue(S, Wk.jb, g);
+                }
+            }
             for (int t = 0; t < ntile && !failed; t++) {
                 const uint32_t gt = g + t;
-                const int rb = gt & 1;
                 const int s = gt % NS;
-                if (lane == 0 && t + 1 < ntile) issue(S, Wk.jb + (t + 1) * TJ, gt + 1);
-                bool ok = mbar_wait_bounded(&bar_raw[rb], (gt >> 1) & 1, WAIT_LIMIT);
-                if (ok && lane == 0) pending[rb] = false;
-                ok = ok && mbar_wait_bounded(&bar_empty[s], ((gt / NS) & 1) ^ 1, WAIT_LIMIT);
+                bool ok = true;
+                if (t + 1 < ntile) {
+                    const uint32_t gn = gt + 1;
+                    ok = mbar_wait_bounded(&bar_empty[gn % NS], ((gn / NS) & 1) ^ 1, WAIT_LIMIT);
+                    if (__all_sync(0xffffffffu, ok) && lane == 0) issue(S, Wk.jb + (t + 1) * TJ, gn);
+                }
+                ok = ok && mbar_wait_bounded(&bar_raw[s], (gt / NS) & 1, WAIT_LIMIT);
+                if (ok && lane == 0) pending[s] = false;
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(a.err, DEVERR_TIMEOUT);
                     failed = true;
                     break;
                 }
                 // rewrite the tile relative to the i-tile centre
-                const float *rbuf = raw + rb * 8 * TJ;
+                const float *rbuf = stage_raw(s);
+                const int rb = s;
                 float *cx = comp + s * 5 * TJ;
 #pragma unroll 4
                 for (int j = lane; j < TJ; j += 32) {
@@ -460,7 +496,9 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                         fold(acc + 3 * NT, acc + 7 * NT, tp[k]);
                     }
                     if (!far) {
-                        // deferred near-field pairs in FP64, in the order found
+                        // deferred near-field pairs in FP64, in the order found; the
+                        // sources' data come from this stage's raw tile
+                        const float *rs = stage_raw(s);
                         for (int e = 0; e < nlist; e++) {
                             const int v = s_near[e * NT + tid];
                             const int kk = v >> 8, j = v & 255;
@@ -468,8 +506,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 #pragma unroll
                             for (int k = 1; k < K; k++)
                                 if (kk == k) ipk = ip[k];
-                            near_fold<NEWTON>(D, a.nkernel, ipk, S.poff + jt + j,
-                                              s_acc + (kk * 8) * NT + tid, NT);
+                            near_fold<NEWTON, TJ>(D, F, a.nkernel, ipk, S.poff + jt + j, rs, j,
+                                                  s_acc + (kk * 8) * NT + tid, NT);
                         }
                         // list overflow: rescan this thread's quads from the overflow
                         // point with the same float test and evaluate every near pair
@@ -490,10 +528,13 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                                     upk(r2, ra, rb);
                                     const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
                                     const int jp0 = S.poff + jt + 4 * qd + 2 * h;
+                                    const int j0 = 4 * qd + 2 * h;
                                     if (ra < fmaxf(h2i[k], ha))
-                                        near_fold<NEWTON>(D, a.nkernel, ip[k], jp0, s_acc + (k * 8) * NT + tid, NT);
+                                        near_fold<NEWTON, TJ>(D, F, a.nkernel, ip[k], jp0, rs, j0,
+                                                              s_acc + (k * 8) * NT + tid, NT);
                                     if (rb < fmaxf(h2i[k], hb))
-                                        near_fold<NEWTON>(D, a.nkernel, ip[k], jp0 + 1, s_acc + (k * 8) * NT + tid, NT);
+                                        near_fold<NEWTON, TJ>(D, F, a.nkernel, ip[k], jp0 + 1, rs, j0 + 1,
+                                                              s_acc + (k * 8) * NT + tid, NT);
                                 }
                             }
                         }
@@ -529,7 +570,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     }
     // never leave with bulk copies in flight into this CTA's shared memory
     if (producer && lane == 0) {
-        for (int b = 0; b < 2; b++)
+        for (int b = 0; b < NS; b++)
             if (pending[b]) mbar_wait_bounded(&bar_raw[b], pend_par[b], WAIT_LIMIT);
     }
 }

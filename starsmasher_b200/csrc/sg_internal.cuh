@@ -82,17 +82,22 @@ __host__ __device__ inline double self_c(int nkernel)
 // particles give -c/2 * flag_{lower original index} * (m_j/H_i + m_j/H_j).
 struct PairOut { double ax, ay, az, pot; };
 
+// The CPU path divides (qq = 1/invq, amj/twohp, mj1/fourhp2); here the same
+// quantities come from reciprocals ih = 1/H = rsqrt(H^2): equal up to a last-
+// bit rounding, at a fraction of the FP64 cost.
 __device__ __forceinline__ void near_kernel_f64(int nkernel, double r2, double rinv,
-                                                double amj, double twohpi, double fourhpi2,
-                                                double twohpj, double fourhpj2,
+                                                double amj, double ihi, double fourhpi2,
+                                                double ihj, double fourhpj2,
                                                 double mrinv1, double mrinv3,
                                                 double &gacc, double &gpot)
 {
+    const double r = r2 * rinv;
+    const double twohpi = fourhpi2 * ihi, twohpj = fourhpj2 * ihj;
     const double invq1 = rinv * twohpi, invq2 = rinv * twohpj;
-    const double qq1 = 1.0 / invq1, qq2 = 1.0 / invq2;
+    const double qq1 = r * ihi, qq2 = r * ihj;
     const double q21 = qq1 * qq1, q22 = qq2 * qq2;
-    const double mj11 = amj / twohpi, mj12 = amj / twohpj;
-    const double mj21 = mj11 / fourhpi2, mj22 = mj12 / fourhpj2;
+    const double mj11 = amj * ihi, mj12 = amj * ihj;
+    const double mj21 = mj11 * (ihi * ihi), mj22 = mj12 * (ihj * ihj);
     const double g1 = (r2 <= fourhpi2) ? 1.0 : 0.0;
     const double g2 = (r2 <= fourhpj2) ? 1.0 : 0.0;
     double acc1, acc2, pot1, pot2;
@@ -136,35 +141,36 @@ __device__ __forceinline__ void near_kernel_f64(int nkernel, double r2, double r
     }
 }
 
-// Full FP64 pair from sorted slots ip (row) and jp (source).
-static __device__ __noinline__ PairOut pair_f64_slots(const SortedF64 D, int nkernel, int ip, int jp)
+// FP64 pair of row slot ip and source slot jp given their separation dr
+// (x_j - x_i), the source mass and both H^2; the zero-distance rule reads
+// the flags and original indices of the sorted layout.
+static __device__ __forceinline__ PairOut pair_f64_core(const SortedF64 &D, int nkernel, int ip,
+                                                        int jp, double dr1, double dr2, double dr3,
+                                                        double amj, double fourhpi2,
+                                                        double fourhpj2)
 {
-    const double xi = D.x[ip], yi = D.y[ip], zi = D.z[ip];
-    const double dr1 = D.x[jp] - xi, dr2 = D.y[jp] - yi, dr3 = D.z[jp] - zi;
     const double r2 = dr1 * dr1 + dr2 * dr2 + dr3 * dr3;
-    const double amj = D.m[jp];
-    const double fourhpi2 = D.h2[ip], fourhpj2 = D.h2[jp];
     double gacc, gpot;
     if (r2 >= fmax(fourhpi2, fourhpj2)) {
-        const double rinv = 1.0 / sqrt(r2);
+        const double rinv = rsqrt(r2);
         const double mrinv1 = rinv * amj;
         gacc = rinv * rinv * mrinv1;
         gpot = -mrinv1;
     } else if (r2 > 0.0) {
-        const double rinv = 1.0 / sqrt(r2);
+        const double rinv = rsqrt(r2);
         const double mrinv1 = rinv * amj;
         const double mrinv3 = rinv * rinv * mrinv1;
-        near_kernel_f64(nkernel, r2, rinv, amj, sqrt(fourhpi2), fourhpi2, sqrt(fourhpj2),
+        near_kernel_f64(nkernel, r2, rinv, amj, rsqrt(fourhpi2), fourhpi2, rsqrt(fourhpj2),
                         fourhpj2, mrinv1, mrinv3, gacc, gpot);
     } else {
         gacc = 0.0;
-        const double twohpi = sqrt(fourhpi2), twohpj = sqrt(fourhpj2);
+        const double s = amj * (rsqrt(fourhpi2) + rsqrt(fourhpj2));  // m/H_i + m/H_j
         const double c = self_c(nkernel);
         if (ip == jp) {
-            gpot = D.flag[ip] ? -c * (amj / twohpi + amj / twohpj) : 0.0;
+            gpot = D.flag[ip] ? -c * s : 0.0;
         } else {
             const int lo = D.orig[ip] < D.orig[jp] ? ip : jp;
-            gpot = D.flag[lo] ? -0.5 * c * (amj / twohpi + amj / twohpj) : 0.0;
+            gpot = D.flag[lo] ? -0.5 * c * s : 0.0;
         }
     }
     PairOut o;
@@ -173,6 +179,14 @@ static __device__ __noinline__ PairOut pair_f64_slots(const SortedF64 D, int nke
     o.az = gacc * dr3;
     o.pot = gpot;
     return o;
+}
+
+// Full FP64 pair from sorted slots ip (row) and jp (source).
+static __device__ __noinline__ PairOut pair_f64_slots(const SortedF64 D, int nkernel, int ip, int jp)
+{
+    const double xi = D.x[ip], yi = D.y[ip], zi = D.z[ip];
+    return pair_f64_core(D, nkernel, ip, jp, D.x[jp] - xi, D.y[jp] - yi, D.z[jp] - zi, D.m[jp],
+                         D.h2[ip], D.h2[jp]);
 }
 
 // ----------------------------------------------------- packed FP32 (sm_100)

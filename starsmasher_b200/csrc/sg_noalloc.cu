@@ -48,7 +48,7 @@ static __device__ __noinline__ PairOut pair_f64_raw(const double *x, const doubl
     } else if (r2 > 0.0) {
         const double rinv = 1.0 / sqrt(r2);
         const double mrinv1 = rinv * amj;
-        near_kernel_f64(nkernel, r2, rinv, amj, sqrt(fourhpi2), fourhpi2, sqrt(fourhpj2),
+        near_kernel_f64(nkernel, r2, rinv, amj, rsqrt(fourhpi2), fourhpi2, rsqrt(fourhpj2),
                         fourhpj2, mrinv1, rinv * rinv * mrinv1, gacc, gpot);
     } else {
         gacc = 0.0;
