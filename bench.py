@@ -375,8 +375,12 @@ def main():
         e = num / amag
         ill = amag < 1e-3 * np.median(amag)
         ep = np.abs(res_f32[3] - res64[3]) / np.abs(res64[3])
+        med = float(np.median(amag))
+        worst = int(np.argmax(np.where(ill, -1.0, e)))
         acc = {"reference": "plain FP64 GPU kernel, all rows",
                "acc_rel_max": float(e[~ill].max()), "acc_rel_rms": float(np.sqrt(np.mean(e[~ill] ** 2))),
+               "acc_abs_max_over_median_a": float(num.max() / med),
+               "worst_particle_a_over_median_a": float(amag[worst] / med),
                "acc_rel_max_illconditioned": float(e[ill].max()) if ill.any() else None,
                "n_illconditioned": int(ill.sum()),
                "pot_rel_max": float(ep.max()), "pot_rel_rms": float(np.sqrt(np.mean(ep ** 2)))}
@@ -395,13 +399,13 @@ def main():
         ctx.profile_enable(False)
     kernel_ms = kern_ms / max(1, kern_n)
     achieved = pairs * FLOPS_PER_PAIR / (kernel_ms * 1e-3) / 1e12
+    # DRAM bytes of one pair-kernel launch on this workload, from a one-pass
+    # ncu capture of this same command (profiles/traffic_*.json), if recorded
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", f"traffic_{args.precision}.json")
+    tfile = os.path.join(ROOT, "profiles", f"traffic_{args.precision}_{args.workload}.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            tb = json.load(f).get("dram_bytes_per_pair")
-        if tb:
-            traffic = tb * pairs
+            traffic = json.load(f).get("dram_bytes_per_launch")
     roofline = {"bound": "fp32-fma", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel_ms_per_launch": kernel_ms, "flops_per_pair": FLOPS_PER_PAIR,

@@ -115,11 +115,10 @@ __device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
 // position pair (a 48-bit representation of the FP64 position, exact in
 // double) and its FP64 mass and H^2; the row's position is rebuilt from its
 // own hi + lo pair so that coincident particles give dr == 0 exactly.
-template <bool NEWTON, int TJ>
-__device__ __noinline__ void near_fold(const SortedF64 D, const SortedF32 F, int nkernel, int ip,
-                                       int jp, const float *rs, int j, float *acc, int stride)
+template <int TJ>
+__device__ __noinline__ PairOut near_pair(const SortedF64 D, const SortedF32 F, int nkernel, int ip,
+                                          int jp, const float *rs, int j)
 {
-    constexpr double SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
     const double *rd = reinterpret_cast<const double *>(rs + 8 * TJ);
     const double xi = (double)F.xh[ip] + (double)F.xl[ip];
     const double yi = (double)F.yh[ip] + (double)F.yl[ip];
@@ -127,8 +126,26 @@ __device__ __noinline__ void near_fold(const SortedF64 D, const SortedF32 F, int
     const double xj = (double)rs[j] + (double)rs[TJ + j];
     const double yj = (double)rs[2 * TJ + j] + (double)rs[3 * TJ + j];
     const double zj = (double)rs[4 * TJ + j] + (double)rs[5 * TJ + j];
-    const PairOut o = pair_f64_core(D, nkernel, ip, jp, xj - xi, yj - yi, zj - zi, rd[j], D.h2[ip],
-                                    rd[TJ + j]);
+    return pair_f64_core(D, nkernel, ip, jp, xj - xi, yj - yi, zj - zi, rd[j], D.h2[ip], rd[TJ + j]);
+}
+
+// Fold an FP64 pair (already in the accumulators' scaled units) into a row's
+// compensated accumulators acc[c * stride] (hi) / acc[(4 + c) * stride] (lo).
+__device__ __forceinline__ void fold_d4(float *acc, int stride, double ax, double ay, double az,
+                                        double pot)
+{
+    ff_add_d(acc[0], acc[4 * stride], ax);
+    ff_add_d(acc[stride], acc[5 * stride], ay);
+    ff_add_d(acc[2 * stride], acc[6 * stride], az);
+    ff_add_d(acc[3 * stride], acc[7 * stride], pot);
+}
+
+template <bool NEWTON, int TJ>
+__device__ __noinline__ void near_fold(const SortedF64 D, const SortedF32 F, int nkernel, int ip,
+                                       int jp, const float *rs, int j, float *acc, int stride)
+{
+    constexpr double SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
+    const PairOut o = near_pair<TJ>(D, F, nkernel, ip, jp, rs, j);
     ff_add_d(acc[0], acc[4 * stride], o.ax / SA);
     ff_add_d(acc[stride], acc[5 * stride], o.ay / SA);
     ff_add_d(acc[2 * stride], acc[6 * stride], o.az / SA);
@@ -156,9 +173,10 @@ struct WsSmem {
     static constexpr int COMP = META + NS * NMETA * 32;    // [NS][5][TJ] floats
     static constexpr int BOX = COMP + NS * 5 * TJ * 4;     // [NS] TileBox
     static constexpr int ACC = BOX + NS * 32;              // [K*8][NT] floats
-    static constexpr int NEARCAP = 32;                     // deferred near pairs per thread
+    static constexpr int NEARCAP = 64;                     // deferred near pairs per thread
     static constexpr int NEAR = ACC + K * 8 * NT * 4;      // [NEARCAP][NT] ushort
-    static constexpr int BAR = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // 3*NS mbarriers
+    static constexpr int NRES = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // [W][32][4] double
+    static constexpr int BAR = NRES + W * 32 * 4 * 8;      // 3*NS mbarriers
     static constexpr int ITEM = BAR + 3 * NS * 8;          // 2 ints
     static constexpr int BYTES = ITEM + 16;
     static constexpr uint32_t TX = RAWSTAGE + NMETA * 32;  // bytes per tile
@@ -187,6 +205,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     TileBox *s_box = reinterpret_cast<TileBox *>(smem + L::BOX);
     float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
     unsigned short *s_near = reinterpret_cast<unsigned short *>(smem + L::NEAR);
+    double *s_res = reinterpret_cast<double *>(smem + L::NRES);
     uint64_t *bar_raw = reinterpret_cast<uint64_t *>(smem + L::BAR);  // [NS]
     uint64_t *bar_full = bar_raw + NS;                                 // [NS]
     uint64_t *bar_empty = bar_full + NS;                               // [NS]
@@ -499,15 +518,52 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                         // deferred near-field pairs in FP64, in the order found; the
                         // sources' data come from this stage's raw tile
                         const float *rs = stage_raw(s);
-                        for (int e = 0; e < nlist; e++) {
-                            const int v = s_near[e * NT + tid];
-                            const int kk = v >> 8, j = v & 255;
-                            int ipk = ip[0];
+                        // The warp's lists, concatenated in lane order, are evaluated
+                        // 32 pairs at a time (one per lane); each owner lane then folds
+                        // its own results in list order, so the sums stay deterministic.
+                        int incl = nlist;
 #pragma unroll
-                            for (int k = 1; k < K; k++)
-                                if (kk == k) ipk = ip[k];
-                            near_fold<NEWTON, TJ>(D, F, a.nkernel, ipk, S.poff + jt + j, rs, j,
-                                                  s_acc + (kk * 8) * NT + tid, NT);
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                            if (lane >= o) incl += v;
+                        }
+                        const int off = incl - nlist;
+                        const int tot = __shfl_sync(0xffffffffu, incl, 31);
+                        double *res = s_res + warp * 32 * 4;
+                        for (int base = 0; base < tot; base += 32) {
+                            const int f = base + lane;
+                            int own = 0;  // largest lane whose list starts at or before f
+#pragma unroll
+                            for (int st = 16; st > 0; st >>= 1) {
+                                const int c = own + st;
+                                const int offc = __shfl_sync(0xffffffffu, off, c & 31);
+                                if (c < 32 && offc <= f) own = c;
+                            }
+                            const int offo = __shfl_sync(0xffffffffu, off, own);
+                            int ipo[K];
+#pragma unroll
+                            for (int k = 0; k < K; k++) ipo[k] = __shfl_sync(0xffffffffu, ip[k], own);
+                            if (f < tot) {
+                                const int v = s_near[(f - offo) * NT + warp * 32 + own];
+                                const int kk = v >> 8, j = v & 255;
+                                int ipk = ipo[0];
+#pragma unroll
+                                for (int k = 1; k < K; k++)
+                                    if (kk == k) ipk = ipo[k];
+                                const PairOut r = near_pair<TJ>(D, F, a.nkernel, ipk, S.poff + jt + j, rs, j);
+                                res[lane * 4 + 0] = r.ax / (double)SA;
+                                res[lane * 4 + 1] = r.ay / (double)SA;
+                                res[lane * 4 + 2] = r.az / (double)SA;
+                                res[lane * 4 + 3] = r.pot / (double)SP;
+                            }
+                            __syncwarp();
+                            const int lo = max(base, off), hi = min(base + 32, off + nlist);
+                            for (int ff = lo; ff < hi; ff++) {
+                                const int kk = s_near[(ff - off) * NT + tid] >> 8;
+                                const double *rr = res + (ff - base) * 4;
+                                fold_d4(s_acc + (kk * 8) * NT + tid, NT, rr[0], rr[1], rr[2], rr[3]);
+                            }
+                            __syncwarp();
                         }
                         // list overflow: rescan this thread's quads from the overflow
                         // point with the same float test and evaluate every near pair
