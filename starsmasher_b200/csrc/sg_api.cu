@@ -326,8 +326,11 @@ static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
         const SetDesc &d = P.sets[0];
         const int jtiles = (d.n + P.tj - 1) / P.tj;
         const int maxch = std::max(1, std::min(jtiles, std::min(64, (int)(((long long)jtiles * P.tj) / kMinChunkJ))));
+        // item costs differ (near-field work is uneven), so small sets want
+        // several items per CTA for the queue to balance them
+        const int nch_min = std::min(maxch, std::max(1, (3 * resident + P.ntiles - 1) / P.ntiles));
         double best = -1.0;
-        for (int nch = 1; nch <= maxch; nch++) {
+        for (int nch = nch_min; nch <= maxch; nch++) {
             const double waves = (double)P.ntiles * nch / resident;
             const double eff = waves / std::ceil(waves) - 0.002 * nch;  // small per-chunk cost
             if (eff > best + 1e-9) { best = eff; single_nch = nch; }

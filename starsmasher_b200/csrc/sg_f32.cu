@@ -113,39 +113,22 @@ __device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
 // in the accumulators' scaled units.
 // The source's data come from the staged raw tile `rs` (index j): the hi + lo
 // position pair (a 48-bit representation of the FP64 position, exact in
-// double) and its FP64 mass and H^2; the row's position is rebuilt from its
-// own hi + lo pair so that coincident particles give dr == 0 exactly.
-template <int TJ>
-__device__ __noinline__ PairOut near_pair(const SortedF64 D, const SortedF32 F, int nkernel, int ip,
-                                          int jp, const float *rs, int j)
+// double) and its FP64 mass and H^2.  The row's data come from the caller's
+// shared-memory row cache `row` = {x, y, z, H^2} (stride `rstride`), its
+// position rebuilt from its own hi + lo pair the same way, so coincident
+// particles give dr == 0 exactly.
+template <bool NEWTON, int TJ>
+__device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, int jp,
+                                       const double *row, int rstride, const float *rs, int j,
+                                       float *acc, int stride)
 {
+    constexpr double SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
     const double *rd = reinterpret_cast<const double *>(rs + 8 * TJ);
-    const double xi = (double)F.xh[ip] + (double)F.xl[ip];
-    const double yi = (double)F.yh[ip] + (double)F.yl[ip];
-    const double zi = (double)F.zh[ip] + (double)F.zl[ip];
     const double xj = (double)rs[j] + (double)rs[TJ + j];
     const double yj = (double)rs[2 * TJ + j] + (double)rs[3 * TJ + j];
     const double zj = (double)rs[4 * TJ + j] + (double)rs[5 * TJ + j];
-    return pair_f64_core(D, nkernel, ip, jp, xj - xi, yj - yi, zj - zi, rd[j], D.h2[ip], rd[TJ + j]);
-}
-
-// Fold an FP64 pair (already in the accumulators' scaled units) into a row's
-// compensated accumulators acc[c * stride] (hi) / acc[(4 + c) * stride] (lo).
-__device__ __forceinline__ void fold_d4(float *acc, int stride, double ax, double ay, double az,
-                                        double pot)
-{
-    ff_add_d(acc[0], acc[4 * stride], ax);
-    ff_add_d(acc[stride], acc[5 * stride], ay);
-    ff_add_d(acc[2 * stride], acc[6 * stride], az);
-    ff_add_d(acc[3 * stride], acc[7 * stride], pot);
-}
-
-template <bool NEWTON, int TJ>
-__device__ __noinline__ void near_fold(const SortedF64 D, const SortedF32 F, int nkernel, int ip,
-                                       int jp, const float *rs, int j, float *acc, int stride)
-{
-    constexpr double SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
-    const PairOut o = near_pair<TJ>(D, F, nkernel, ip, jp, rs, j);
+    const PairOut o = pair_f64_core(D, nkernel, ip, jp, xj - row[0], yj - row[rstride],
+                                    zj - row[2 * rstride], rd[j], row[3 * rstride], rd[TJ + j]);
     ff_add_d(acc[0], acc[4 * stride], o.ax / SA);
     ff_add_d(acc[stride], acc[5 * stride], o.ay / SA);
     ff_add_d(acc[2 * stride], acc[6 * stride], o.az / SA);
@@ -173,10 +156,10 @@ struct WsSmem {
     static constexpr int COMP = META + NS * NMETA * 32;    // [NS][5][TJ] floats
     static constexpr int BOX = COMP + NS * 5 * TJ * 4;     // [NS] TileBox
     static constexpr int ACC = BOX + NS * 32;              // [K*8][NT] floats
-    static constexpr int NEARCAP = 64;                     // deferred near pairs per thread
+    static constexpr int NEARCAP = 32;                     // deferred near pairs per thread
     static constexpr int NEAR = ACC + K * 8 * NT * 4;      // [NEARCAP][NT] ushort
-    static constexpr int NRES = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // [W][32][4] double
-    static constexpr int BAR = NRES + W * 32 * 4 * 8;      // 3*NS mbarriers
+    static constexpr int ROW = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // [K][4][NT] double
+    static constexpr int BAR = ROW + K * 4 * NT * 8;       // 3*NS mbarriers
     static constexpr int ITEM = BAR + 3 * NS * 8;          // 2 ints
     static constexpr int BYTES = ITEM + 16;
     static constexpr uint32_t TX = RAWSTAGE + NMETA * 32;  // bytes per tile
@@ -205,7 +188,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     TileBox *s_box = reinterpret_cast<TileBox *>(smem + L::BOX);
     float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
     unsigned short *s_near = reinterpret_cast<unsigned short *>(smem + L::NEAR);
-    double *s_res = reinterpret_cast<double *>(smem + L::NRES);
+    double *s_row = reinterpret_cast<double *>(smem + L::ROW);  // [K][4][NT]: x y z H^2
     uint64_t *bar_raw = reinterpret_cast<uint64_t *>(smem + L::BAR);  // [NS]
     uint64_t *bar_full = bar_raw + NS;                                 // [NS]
     uint64_t *bar_empty = bar_full + NS;                               // [NS]
@@ -359,6 +342,12 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     y = __fadd_rn(__fsub_rn(F.yh[sl], C.chy), __fsub_rn(F.yl[sl], C.cly));
                     z = __fadd_rn(__fsub_rn(F.zh[sl], C.chz), __fsub_rn(F.zl[sl], C.clz));
                     h2 = FP64_BAND2 * F.h2[sl];
+                    // FP64 row data for the deferred near pairs
+                    double *rw = s_row + (k * 4) * NT + tid;
+                    rw[0] = (double)F.xh[sl] + (double)F.xl[sl];
+                    rw[NT] = (double)F.yh[sl] + (double)F.yl[sl];
+                    rw[2 * NT] = (double)F.zh[sl] + (double)F.zl[sl];
+                    rw[3 * NT] = D.h2[sl];
                     wlo[0] = fminf(wlo[0], x); whi[0] = fmaxf(whi[0], x);
                     wlo[1] = fminf(wlo[1], y); whi[1] = fmaxf(whi[1], y);
                     wlo[2] = fminf(wlo[2], z); whi[2] = fmaxf(whi[2], z);
@@ -518,52 +507,16 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                         // deferred near-field pairs in FP64, in the order found; the
                         // sources' data come from this stage's raw tile
                         const float *rs = stage_raw(s);
-                        // The warp's lists, concatenated in lane order, are evaluated
-                        // 32 pairs at a time (one per lane); each owner lane then folds
-                        // its own results in list order, so the sums stay deterministic.
-                        int incl = nlist;
+                        for (int e = 0; e < nlist; e++) {
+                            const int v = s_near[e * NT + tid];
+                            const int kk = v >> 8, j = v & 255;
+                            int ipk = ip[0];
 #pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                            if (lane >= o) incl += v;
-                        }
-                        const int off = incl - nlist;
-                        const int tot = __shfl_sync(0xffffffffu, incl, 31);
-                        double *res = s_res + warp * 32 * 4;
-                        for (int base = 0; base < tot; base += 32) {
-                            const int f = base + lane;
-                            int own = 0;  // largest lane whose list starts at or before f
-#pragma unroll
-                            for (int st = 16; st > 0; st >>= 1) {
-                                const int c = own + st;
-                                const int offc = __shfl_sync(0xffffffffu, off, c & 31);
-                                if (c < 32 && offc <= f) own = c;
-                            }
-                            const int offo = __shfl_sync(0xffffffffu, off, own);
-                            int ipo[K];
-#pragma unroll
-                            for (int k = 0; k < K; k++) ipo[k] = __shfl_sync(0xffffffffu, ip[k], own);
-                            if (f < tot) {
-                                const int v = s_near[(f - offo) * NT + warp * 32 + own];
-                                const int kk = v >> 8, j = v & 255;
-                                int ipk = ipo[0];
-#pragma unroll
-                                for (int k = 1; k < K; k++)
-                                    if (kk == k) ipk = ipo[k];
-                                const PairOut r = near_pair<TJ>(D, F, a.nkernel, ipk, S.poff + jt + j, rs, j);
-                                res[lane * 4 + 0] = r.ax / (double)SA;
-                                res[lane * 4 + 1] = r.ay / (double)SA;
-                                res[lane * 4 + 2] = r.az / (double)SA;
-                                res[lane * 4 + 3] = r.pot / (double)SP;
-                            }
-                            __syncwarp();
-                            const int lo = max(base, off), hi = min(base + 32, off + nlist);
-                            for (int ff = lo; ff < hi; ff++) {
-                                const int kk = s_near[(ff - off) * NT + tid] >> 8;
-                                const double *rr = res + (ff - base) * 4;
-                                fold_d4(s_acc + (kk * 8) * NT + tid, NT, rr[0], rr[1], rr[2], rr[3]);
-                            }
-                            __syncwarp();
+                            for (int k = 1; k < K; k++)
+                                if (kk == k) ipk = ip[k];
+                            near_fold<NEWTON, TJ>(D, a.nkernel, ipk, S.poff + jt + j,
+                                                  s_row + (kk * 4) * NT + tid, NT, rs, j,
+                                                  s_acc + (kk * 8) * NT + tid, NT);
                         }
                         // list overflow: rescan this thread's quads from the overflow
                         // point with the same float test and evaluate every near pair
@@ -586,10 +539,12 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                                     const int jp0 = S.poff + jt + 4 * qd + 2 * h;
                                     const int j0 = 4 * qd + 2 * h;
                                     if (ra < fmaxf(h2i[k], ha))
-                                        near_fold<NEWTON, TJ>(D, F, a.nkernel, ip[k], jp0, rs, j0,
+                                        near_fold<NEWTON, TJ>(D, a.nkernel, ip[k], jp0,
+                                                              s_row + (k * 4) * NT + tid, NT, rs, j0,
                                                               s_acc + (k * 8) * NT + tid, NT);
                                     if (rb < fmaxf(h2i[k], hb))
-                                        near_fold<NEWTON, TJ>(D, F, a.nkernel, ip[k], jp0 + 1, rs, j0 + 1,
+                                        near_fold<NEWTON, TJ>(D, a.nkernel, ip[k], jp0 + 1,
+                                                              s_row + (k * 4) * NT + tid, NT, rs, j0 + 1,
                                                               s_acc + (k * 8) * NT + tid, NT);
                                 }
                             }
