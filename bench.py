@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--variant", type=int, default=-1,
                    help="force a kernel variant of --precision (default: tuned/automatic)")
+    p.add_argument("--fp64-band", type=float, default=2.0,
+                   help="split-FP32: pairs with r < band * max(H) are evaluated in FP64")
     p.add_argument("--graph", action="store_true",
                    help="batched workloads: each step replays a captured CUDA graph of "
                         "(seeded 1e-3 position kick + gravity) on device-resident state")
@@ -247,6 +249,7 @@ def main():
     ctx.set_stream(stream.cuda_stream)
     if args.variant >= 0:
         ctx.force_variant(args.precision, args.variant)
+    ctx.set_fp64_band(args.fp64_band)
 
     dt = torch.float64
     X = [torch.as_tensor(a).to(device=f"cuda:{device}", dtype=dt)
@@ -458,6 +461,7 @@ def main():
             "data": "synthetic: seeded polytropic star models (no public dataset), one independent model per rank",
             "config": {"workload": ws.name, "n": n, "nsets": ws.nsets, "pairs_per_step": pairs,
                        "precision": args.precision, "nkernel": args.nkernel,
+                       "fp64_band": args.fp64_band,
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"replicas x{world} (independent models per GPU)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,

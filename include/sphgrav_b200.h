@@ -183,6 +183,12 @@ int sphgrav_autotune(sphgrav_ctx *ctx, int nsets, const int *offsets,
 /* Persist / restore the tuning table (a small JSON file). */
 int sphgrav_tuning_save(sphgrav_ctx *ctx, const char *path);
 int sphgrav_tuning_load(sphgrav_ctx *ctx, const char *path);
+/* Split-FP32 only: pairs with r < factor * max(H_i, H_j) are evaluated in
+ * FP64 (default 2.0; 1.0 = only the softened near field, r < max H).  A wider
+ * band lowers the error of particles whose acceleration cancels and costs
+ * time in proportion to the pairs it moves (~factor^3 times the near-field
+ * pairs).  Factor in [1, 16].  No reference counterpart. */
+int sphgrav_set_fp64_band(sphgrav_ctx *ctx, double factor);
 /* Force a kernel variant by index (-1 = automatic) for a precision. */
 int sphgrav_force_variant(sphgrav_ctx *ctx, int precision, int variant);
 /* Number of kernel variants and a printable name of each. */

@@ -56,6 +56,7 @@ SIGNATURES = {
     "sphgrav_tuning_save": (_I, [_P, ctypes.c_char_p]),
     "sphgrav_tuning_load": (_I, [_P, ctypes.c_char_p]),
     "sphgrav_force_variant": (_I, [_P, _I, _I]),
+    "sphgrav_set_fp64_band": (_I, [_P, _D]),
     "sphgrav_variant_count": (_I, [_I]),
     "sphgrav_variant_name": (ctypes.c_char_p, [_I, _I]),
     "sphgrav_status_string": (ctypes.c_char_p, [_I]),

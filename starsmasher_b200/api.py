@@ -115,6 +115,10 @@ class Context:
         check(self._lib.sphgrav_force_variant(self._h, _prec(precision), int(variant)),
               "sphgrav_force_variant")
 
+    def set_fp64_band(self, factor: float) -> None:
+        """Split-FP32: evaluate pairs with r < factor * max(H) in FP64 (default 2)."""
+        check(self._lib.sphgrav_set_fp64_band(self._h, float(factor)), "sphgrav_set_fp64_band")
+
     def plan_info(self) -> dict:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(self._lib.sphgrav_last_plan_info(self._h, ctypes.byref(a), ctypes.byref(b),

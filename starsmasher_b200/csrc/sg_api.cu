@@ -184,6 +184,7 @@ struct sphgrav_ctx {
     std::map<int, std::string> tuned[2];  // N bucket -> variant name
 
     // kernel timing (sphgrav_profile_*)
+    double fp64_band = 2.0;  // split-FP32: FP64 for r < fp64_band * max(H)
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
@@ -525,6 +526,7 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     a.err = c->err.p;
     a.nkernel = nkernel;
     a.itile = P.itile;
+    a.band2 = (float)(c->fp64_band * c->fp64_band);
     const bool timed = c->profiling && !c->capturing && P.nitems > 0;
     if (timed) {
         if (c->prof_used == c->prof_events.size()) {
@@ -1069,6 +1071,15 @@ int sphgrav_last_plan_info(sphgrav_ctx *c, int *nitems, int *nchunks_max, int *v
     if (nitems) *nitems = c->plan.nitems;
     if (nchunks_max) *nchunks_max = c->plan.nchunks_max;
     if (variant) *variant = c->plan.variant;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_set_fp64_band(sphgrav_ctx *c, double factor)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (!(factor >= 1.0 && factor <= 16.0))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "fp64 band factor %g outside [1, 16]", factor);
+    c->fp64_band = factor;
     return SPHGRAV_OK;
 }
 

@@ -36,7 +36,7 @@
 //     the CPU-path formulas) after the tile's FP32 loop and folded into the
 //     same accumulators: below H the softened near field, whose reference
 //     polynomials cancel by up to ~1e3 near q = 1, and between H and 2H the
-//     largest Newtonian terms (see FP64_BAND2).  A warp skips the per-pair
+//     largest Newtonian terms (see ComputeArgs::band2).  A warp skips the per-pair
 //     test for a tile when the bounding boxes of its rows and of the tile are
 //     farther apart than 2 max(H) of both.
 //   * per (row, j-chunk) results leave the CTA as FP64 partial sums merged in
@@ -135,13 +135,15 @@ __device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, i
     ff_add_d(acc[3 * stride], acc[7 * stride], o.pot / SP);
 }
 
-// Pairs with r^2 < FP64_BAND2 * max(H_i^2, H_j^2), i.e. r < 2 max(H), take the
-// FP64 path.  Below H that is the softened near field (reference polynomials,
-// which cancel in FP32); between H and 2H it is the Newtonian term in FP64:
-// these are the largest far-field terms, and in FP32 their rounding alone
-// sets a ~1e-6 floor on the relative error of a particle whose acceleration
-// cancels (|a| ~ 0.05 max), while they are only ~1e-3 of all pairs at N=1M.
-constexpr float FP64_BAND2 = 4.0f;
+// Pairs with r < band * max(H_i, H_j) take the FP64 path (ComputeArgs::band2 =
+// band^2, >= 1; default band 2).  Below H that is the softened near field
+// (reference polynomials, which cancel in FP32); between H and band*H it is
+// the Newtonian term in FP64: these are the largest far-field terms, and in
+// FP32 their rounding alone sets a ~1e-6 floor on the relative error of a
+// particle whose acceleration cancels (|a| ~ 0.05 median), while at band 2
+// they are only ~1e-3 of all pairs at N=1M.  Scaling H^2 by band2 only moves
+// pairs between two correct evaluations; with band2 >= 1 every r < H pair
+// stays on the FP64 path.
 
 // Shared-memory layout of one CTA (dynamic shared memory, byte offsets).
 template <int W, int K, int TJ, int NS>
@@ -291,7 +293,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     cx[2 * TJ + j] = __fadd_rn(__fsub_rn(rbuf[4 * TJ + j], C.chz),
                                                __fsub_rn(rbuf[5 * TJ + j], C.clz));
                     cx[3 * TJ + j] = rbuf[6 * TJ + j];
-                    cx[4 * TJ + j] = FP64_BAND2 * rbuf[7 * TJ + j];  // (2H)^2: exact scaling
+                    cx[4 * TJ + j] = a.band2 * rbuf[7 * TJ + j];  // (band H)^2
                 }
                 if (lane == 0) {
                     TileBox B;
@@ -313,7 +315,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                             B.lo[d] = fminf(B.lo[d], rc - e);
                             B.hi[d] = fmaxf(B.hi[d], rc + e);
                         }
-                        B.h2max = fmaxf(B.h2max, FP64_BAND2 * M.h2max);
+                        B.h2max = fmaxf(B.h2max, a.band2 * M.h2max * 1.000001f);
                     }
                     s_box[s] = B;
                 }
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     x = __fadd_rn(__fsub_rn(F.xh[sl], C.chx), __fsub_rn(F.xl[sl], C.clx));
                     y = __fadd_rn(__fsub_rn(F.yh[sl], C.chy), __fsub_rn(F.yl[sl], C.cly));
                     z = __fadd_rn(__fsub_rn(F.zh[sl], C.chz), __fsub_rn(F.zl[sl], C.clz));
-                    h2 = FP64_BAND2 * F.h2[sl];
+                    h2 = a.band2 * F.h2[sl];
                     // FP64 row data for the deferred near pairs
                     double *rw = s_row + (k * 4) * NT + tid;
                     rw[0] = (double)F.xh[sl] + (double)F.xl[sl];

@@ -59,6 +59,7 @@ struct ComputeArgs {
     int *err;
     int nkernel;
     int itile;
+    float band2;         // split-FP32: pairs with r^2 < band2 * max(H^2) use FP64 (>= 1)
 };
 
 struct VariantInfo {

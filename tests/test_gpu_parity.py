@@ -234,3 +234,27 @@ def test_red_giant_core_subset(gpu_ctx):
     g = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "fp64")
     r64 = err_report(*(a[rows] for a in g), *o)
     assert r64["acc_max"] <= FP64_TOL and r64["pot_max"] <= FP64_TOL, r64
+
+
+@pytest.mark.parametrize("band", [1.0, 1.5, 3.0])
+def test_fp64_band_setting(gpu_ctx, star16k, tri16k, band):
+    """sphgrav_set_fp64_band moves pairs between two correct evaluations: every
+    setting stays accurate (band 1 keeps only the softened near field in FP64,
+    so its worst, cancellation-dominated particle may exceed 1e-6)."""
+    s = star16k
+    try:
+        gpu_ctx.set_fp64_band(band)
+        got = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
+    finally:
+        gpu_ctx.set_fp64_band(2.0)
+    r = err_report(*got, *tri16k[0])
+    print("band", band, r)
+    assert r["acc_rms"] <= 1e-7 and r["pot_max"] <= F32_TOL
+    assert r["acc_max"] <= (3 * F32_TOL if band < 2.0 else F32_TOL), r
+
+
+def test_fp64_band_rejects_bad_values(gpu_ctx):
+    for bad in (0.5, 0.0, -1.0, 100.0, float("nan")):
+        with pytest.raises(_lib.SphgravError) as e:
+            gpu_ctx.set_fp64_band(bad)
+        assert e.value.status == _lib.ERR_INVALID_ARGUMENT
