@@ -117,22 +117,102 @@ __device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
 // shared-memory row cache `row` = {x, y, z, H^2} (stride `rstride`), its
 // position rebuilt from its own hi + lo pair the same way, so coincident
 // particles give dr == 0 exactly.
-template <bool NEWTON, int TJ>
-__device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, int jp,
-                                       const double *row, int rstride, const float *rs, int j,
-                                       float *acc, int stride)
+// Warp-cooperative FP64 evaluation of the near pairs (r < band * max H) that
+// the checked loop flagged for one staged j-tile.  Each thread holds one 16-bit
+// mask per (row k, sub-block sb) of its sources (bit = 4u + 2h + e for source
+// j = 4 (phase + (sb*SUBQ + u) Q) + 2h + e, the checked loop's order); `wsum`
+// marks its non-empty masks.  Per mask index (uniform over the warp) the set
+// bits of all lanes are compacted into `cbuf` in lane order, evaluated one
+// pair per lane (the row's data from the FP64 row cache of the owning thread,
+// the source's from the raw staged tile: hi + lo position pair, FP64 m, H^2),
+// and every owner sums its own results in list order in FP64, then folds the
+// sums once per row into its compensated accumulators: deterministic, and
+// all lanes busy whatever the distribution of near pairs over the rows.
+template <int K, int Q, int TJ, int NT, bool NEWTON>
+__device__ __noinline__ void near_eval(const SortedF64 D, int nkernel, int jbase, int ip0,
+                                       int ip1, uint32_t wsum, const unsigned short *nbits,
+                                       const double *s_row, float *s_acc, const float *rs,
+                                       unsigned short *cbuf, double *res)
 {
+    constexpr int SUBQ = 4;
+    constexpr int NSB = TJ / (16 * Q);
     constexpr double SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, wb = tid - lane;
     const double *rd = reinterpret_cast<const double *>(rs + 8 * TJ);
-    const double xj = (double)rs[j] + (double)rs[TJ + j];
-    const double yj = (double)rs[2 * TJ + j] + (double)rs[3 * TJ + j];
-    const double zj = (double)rs[4 * TJ + j] + (double)rs[5 * TJ + j];
-    const PairOut o = pair_f64_core(D, nkernel, ip, jp, xj - row[0], yj - row[rstride],
-                                    zj - row[2 * rstride], rd[j], row[3 * rstride], rd[TJ + j]);
-    ff_add_d(acc[0], acc[4 * stride], o.ax / SA);
-    ff_add_d(acc[stride], acc[5 * stride], o.ay / SA);
-    ff_add_d(acc[2 * stride], acc[6 * stride], o.az / SA);
-    ff_add_d(acc[3 * stride], acc[7 * stride], o.pot / SP);
+    uint32_t rem = __reduce_or_sync(FULL, wsum);
+    int kcur = -1;
+    double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+    auto fold_row = [&]() {
+        if (sx != 0.0 || sy != 0.0 || sz != 0.0 || sp != 0.0) {
+            float *acc = s_acc + (kcur * 8) * NT + tid;
+            ff_add_d(acc[0], acc[4 * NT], sx / SA);
+            ff_add_d(acc[NT], acc[5 * NT], sy / SA);
+            ff_add_d(acc[2 * NT], acc[6 * NT], sz / SA);
+            ff_add_d(acc[3 * NT], acc[7 * NT], sp / SP);
+        }
+    };
+    while (rem) {
+        const int wd = __ffs(rem) - 1;
+        rem &= rem - 1;
+        const int k = wd / NSB, sb = wd - k * NSB;
+        if (k != kcur) {
+            if (kcur >= 0) fold_row();
+            kcur = k;
+            sx = sy = sz = sp = 0.0;
+        }
+        const uint32_t m = ((wsum >> wd) & 1u) ? (uint32_t)nbits[wd * NT + tid] : 0u;
+        const int c = __popc(m);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        const int excl = incl - c;
+        {
+            uint32_t mm = m;
+            for (int p = excl; mm; p++) {
+                const int b = __ffs(mm) - 1;
+                mm &= mm - 1;
+                cbuf[p] = (unsigned short)((lane << 4) | b);
+            }
+        }
+        __syncwarp();
+        const int ipk = (K > 1 && k) ? ip1 : ip0;
+        const double *rowk = s_row + (k * 4) * NT + wb;
+        for (int base = 0; base < total; base += 32) {
+            const int g = base + lane;
+            const int ent = g < total ? (int)cbuf[g] : lane << 4;
+            const int ow = ent >> 4, bit = ent & 15;
+            const int ipo = __shfl_sync(FULL, ipk, ow);
+            if (g < total) {
+                const int j = 4 * ((ow % Q) + (sb * SUBQ + (bit >> 2)) * Q) + (bit & 3);
+                const double *row = rowk + ow;
+                const double xj = (double)rs[j] + (double)rs[TJ + j];
+                const double yj = (double)rs[2 * TJ + j] + (double)rs[3 * TJ + j];
+                const double zj = (double)rs[4 * TJ + j] + (double)rs[5 * TJ + j];
+                const PairOut o = pair_f64_core(D, nkernel, ipo, jbase + j, xj - row[0],
+                                                yj - row[NT], zj - row[2 * NT], rd[j], row[3 * NT],
+                                                rd[TJ + j]);
+                res[lane] = o.ax;
+                res[32 + lane] = o.ay;
+                res[64 + lane] = o.az;
+                res[96 + lane] = o.pot;
+            }
+            __syncwarp();
+            const int e1 = min(incl, base + 32);
+            for (int e = max(excl, base); e < e1; e++) {
+                sx += res[e - base];
+                sy += res[32 + e - base];
+                sz += res[64 + e - base];
+                sp += res[96 + e - base];
+            }
+            __syncwarp();
+        }
+    }
+    if (kcur >= 0) fold_row();
 }
 
 // Pairs with r < band * max(H_i, H_j) take the FP64 path (ComputeArgs::band2 =
@@ -146,7 +226,7 @@ __device__ __noinline__ void near_fold(const SortedF64 D, int nkernel, int ip, i
 // stays on the FP64 path.
 
 // Shared-memory layout of one CTA (dynamic shared memory, byte offsets).
-template <int W, int K, int TJ, int NS>
+template <int W, int K, int Q, int TJ, int NS>
 struct WsSmem {
     static constexpr int NT = W * 32;
     static constexpr int NMETA = TJ / META_J;
@@ -158,9 +238,12 @@ struct WsSmem {
     static constexpr int COMP = META + NS * NMETA * 32;    // [NS][5][TJ] floats
     static constexpr int BOX = COMP + NS * 5 * TJ * 4;     // [NS] TileBox
     static constexpr int ACC = BOX + NS * 32;              // [K*8][NT] floats
-    static constexpr int NEARCAP = 32;                     // deferred near pairs per thread
-    static constexpr int NEAR = ACC + K * 8 * NT * 4;      // [NEARCAP][NT] ushort
-    static constexpr int ROW = NEAR + (NEARCAP * NT * 2 + 15) / 16 * 16;  // [K][4][NT] double
+    static constexpr int NSB = TJ / (16 * Q);              // 16-source sub-blocks per thread
+    static constexpr int NBITS = ACC + K * 8 * NT * 4;     // [K*NSB][NT] ushort near masks
+    static constexpr int COOP = NBITS + (K * NSB * NT * 2 + 15) / 16 * 16;  // [W] near_eval buffers
+    static constexpr int COOP_RES = 128 * 8;               // per warp: 4 x 32 doubles ...
+    static constexpr int COOP_BUF = 32 * 16 * 2;           // ... and up to 32 x 16 entries
+    static constexpr int ROW = COOP + W * (COOP_RES + COOP_BUF);  // [K][4][NT] double
     static constexpr int BAR = ROW + K * 4 * NT * 8;       // 3*NS mbarriers
     static constexpr int ITEM = BAR + 3 * NS * 8;          // 2 ints
     static constexpr int BYTES = ITEM + 16;
@@ -174,22 +257,23 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     constexpr int SUBQ = 4;                // quads per sub-block (8 sources per lane)
     static_assert((TJ / 4) % (Q * SUBQ) == 0, "j-tile must hold whole sub-blocks");
     static_assert(TJ % 32 == 0, "producer lanes split the tile");
-    using L = WsSmem<W, K, TJ, NS>;
+    using L = WsSmem<W, K, Q, TJ, NS>;
     constexpr int NT = L::NT;              // consumer threads
     constexpr int RPW = 32 / Q;            // row groups per warp
     constexpr int ITILE = NT * K / Q;      // rows per i-tile
     constexpr int NMETA = L::NMETA;
     constexpr float SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
     constexpr uint32_t WAIT_LIMIT = 1u << 22;
-    constexpr int NOVF = TJ / 4;           // "no overflow" marker of the near list
-    constexpr int NEARCAP = L::NEARCAP;
+    constexpr int NSB = L::NSB;
+    static_assert(K * NSB <= 32, "one summary bit per near mask");
+    static_assert(K <= 2, "near_eval takes the row slots of at most two rows");
 
     extern __shared__ __align__(128) unsigned char smem[];
     JMeta *s_meta = reinterpret_cast<JMeta *>(smem + L::META);
     float *comp = reinterpret_cast<float *>(smem + L::COMP);
     TileBox *s_box = reinterpret_cast<TileBox *>(smem + L::BOX);
     float *s_acc = reinterpret_cast<float *>(smem + L::ACC);
-    unsigned short *s_near = reinterpret_cast<unsigned short *>(smem + L::NEAR);
+    unsigned short *s_nbits = reinterpret_cast<unsigned short *>(smem + L::NBITS);
     double *s_row = reinterpret_cast<double *>(smem + L::ROW);  // [K][4][NT]: x y z H^2
     uint64_t *bar_raw = reinterpret_cast<uint64_t *>(smem + L::BAR);  // [NS]
     uint64_t *bar_full = bar_raw + NS;                                 // [NS]
@@ -405,7 +489,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     f2 tx[K], ty[K], tz[K], tp[K];
 #pragma unroll
                     for (int k = 0; k < K; k++) tx[k] = ty[k] = tz[k] = tp[k] = pk(0.f, 0.f);
-                    int nlist = 0, ovf = NOVF;
+                    uint32_t wsum = 0;  // non-empty near masks of this thread (bit k*NSB + sb)
 
                     if (far) {
                         for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
@@ -437,15 +521,18 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                             }
                         }
                     } else {
-                        // near pairs are masked here and recorded (row k, source j)
-                        // in this thread's list; FP64 evaluation runs after the loop
-                        for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
+                        // near pairs are masked here and flagged in this thread's
+                        // per-(row, sub-block) masks; FP64 evaluation runs after the loop
+                        for (int base = phase, sb = 0; base < TJ / 4; base += Q * SUBQ, sb++) {
                             f2 ax[K], ay[K], az[K], pp[K];
+                            uint32_t mb[K];
 #pragma unroll
-                            for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
+                            for (int k = 0; k < K; k++) {
+                                ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
+                                mb[k] = 0u;
+                            }
                             for (int u = 0; u < SUBQ; u++) {
                                 const int qd = base + u * Q;
-                                const int n0 = nlist;
                                 const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
                                 const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
                                 const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
@@ -465,20 +552,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                                         const bool na = ra < fmaxf(h2i[k], ha);
                                         const bool nb = rb < fmaxf(h2i[k], hb);
                                         if (na || nb) {
-                                            if (ovf == NOVF && act[k]) {
-                                                const int j0 = 4 * qd + 2 * h;
-                                                if (na) {
-                                                    if (nlist < NEARCAP) s_near[nlist * NT + tid] = (k << 8) | j0;
-                                                    else ovf = qd;
-                                                    nlist++;
-                                                }
-                                                if (nb) {
-                                                    if (nlist < NEARCAP) s_near[nlist * NT + tid] = (k << 8) | (j0 + 1);
-                                                    else ovf = qd;
-                                                    nlist++;
-                                                }
-                                                if (ovf != NOVF) nlist = n0;  // the rescan redoes this quad
-                                            }
+                                            mb[k] |= ((na ? 1u : 0u) | (nb ? 2u : 0u)) << (4 * u + 2 * h);
                                             float ma, mb;
                                             upk(mj, ma, mb);
                                             mj = pk(na ? 0.f : ma, nb ? 0.f : mb);
@@ -494,6 +568,10 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                                 ty[k] = add2(ty[k], ay[k]);
                                 tz[k] = add2(tz[k], az[k]);
                                 tp[k] = add2(tp[k], pp[k]);
+                                if (act[k] && mb[k]) {
+                                    s_nbits[(k * NSB + sb) * NT + tid] = (unsigned short)mb[k];
+                                    wsum |= 1u << (k * NSB + sb);
+                                }
                             }
                         }
                     }
@@ -505,52 +583,14 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                         fold(acc + 2 * NT, acc + 6 * NT, tz[k]);
                         fold(acc + 3 * NT, acc + 7 * NT, tp[k]);
                     }
-                    if (!far) {
-                        // deferred near-field pairs in FP64, in the order found; the
-                        // sources' data come from this stage's raw tile
-                        const float *rs = stage_raw(s);
-                        for (int e = 0; e < nlist; e++) {
-                            const int v = s_near[e * NT + tid];
-                            const int kk = v >> 8, j = v & 255;
-                            int ipk = ip[0];
-#pragma unroll
-                            for (int k = 1; k < K; k++)
-                                if (kk == k) ipk = ip[k];
-                            near_fold<NEWTON, TJ>(D, a.nkernel, ipk, S.poff + jt + j,
-                                                  s_row + (kk * 4) * NT + tid, NT, rs, j,
-                                                  s_acc + (kk * 8) * NT + tid, NT);
-                        }
-                        // list overflow: rescan this thread's quads from the overflow
-                        // point with the same float test and evaluate every near pair
-                        for (int qd = ovf; qd < TJ / 4; qd += Q) {
-                            const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
-                            const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
-                            const ulonglong2 Z = *reinterpret_cast<const ulonglong2 *>(&s_z[4 * qd]);
-                            const float4 H = *reinterpret_cast<const float4 *>(&s_h[4 * qd]);
-#pragma unroll
-                            for (int k = 0; k < K; k++) {
-                                if (!act[k]) continue;
-#pragma unroll
-                                for (int h = 0; h < 2; h++) {
-                                    f2 dx, dy, dz, r2;
-                                    geom2(h ? X.y : X.x, h ? Y.y : Y.x, h ? Z.y : Z.x, xi[k], yi[k],
-                                          zi[k], dx, dy, dz, r2);
-                                    float ra, rb;
-                                    upk(r2, ra, rb);
-                                    const float ha = h ? H.z : H.x, hb = h ? H.w : H.y;
-                                    const int jp0 = S.poff + jt + 4 * qd + 2 * h;
-                                    const int j0 = 4 * qd + 2 * h;
-                                    if (ra < fmaxf(h2i[k], ha))
-                                        near_fold<NEWTON, TJ>(D, a.nkernel, ip[k], jp0,
-                                                              s_row + (k * 4) * NT + tid, NT, rs, j0,
-                                                              s_acc + (k * 8) * NT + tid, NT);
-                                    if (rb < fmaxf(h2i[k], hb))
-                                        near_fold<NEWTON, TJ>(D, a.nkernel, ip[k], jp0 + 1,
-                                                              s_row + (k * 4) * NT + tid, NT, rs, j0 + 1,
-                                                              s_acc + (k * 8) * NT + tid, NT);
-                                }
-                            }
-                        }
+                    // deferred near-field pairs in FP64 (far is uniform over the warp)
+                    if (!far && __any_sync(0xffffffffu, wsum != 0u)) {
+                        unsigned char *cb = smem + L::COOP + warp * (L::COOP_RES + L::COOP_BUF);
+                        near_eval<K, Q, TJ, NT, NEWTON>(
+                            D, a.nkernel, S.poff + jt, ip[0], ip[K > 1 ? K - 1 : 0], wsum, s_nbits,
+                            s_row, s_acc, stage_raw(s),
+                            reinterpret_cast<unsigned short *>(cb + L::COOP_RES),
+                            reinterpret_cast<double *>(cb));
                     }
                 }
                 mbar_arrive(&bar_empty[s]);
@@ -603,7 +643,7 @@ static const VariantInfo kF32Variants[] = {SG_F32_VARIANTS(SG_INFO)};
 #define SG_PTR(W, K, Q, TJ, NS, NW, NAME) (const void *)k_f32split<W, K, Q, TJ, NS, NW>,
 static const void *kF32Kernels[] = {SG_F32_VARIANTS(SG_PTR)};
 #undef SG_PTR
-#define SG_SMEM(W, K, Q, TJ, NS, NW, NAME) WsSmem<W, K, TJ, NS>::BYTES,
+#define SG_SMEM(W, K, Q, TJ, NS, NW, NAME) WsSmem<W, K, Q, TJ, NS>::BYTES,
 static const int kF32Smem[] = {SG_F32_VARIANTS(SG_SMEM)};
 #undef SG_SMEM
 constexpr int kNF32 = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
@@ -632,7 +672,7 @@ cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st)
     int idx = 0;
 #define SG_CASE(W, K, Q, TJ, NS, NW, NAME)                                                    \
     if (v == idx) {                                                                           \
-        k_f32split<W, K, Q, TJ, NS, NW><<<grid, (W + 1) * 32, WsSmem<W, K, TJ, NS>::BYTES, st>>>(a); \
+        k_f32split<W, K, Q, TJ, NS, NW><<<grid, (W + 1) * 32, WsSmem<W, K, Q, TJ, NS>::BYTES, st>>>(a); \
         ++g_launches;                                                                         \
         return cudaGetLastError();                                                            \
     }                                                                                         \
