@@ -267,9 +267,11 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
         if (v >= 0) return v;
     }
     if (precision == SPHGRAV_FP64) return 0;
-    // defaults by pair-weighted mean N: wide i-tiles for large sets, several
-    // threads per row for small ones (more CTAs, shorter tiles per thread)
-    if (b >= 15) return 0;
+    // defaults by pair-weighted mean N (measured on B200): two rows per
+    // thread from 2^18 on, two threads per row for 2^13..2^18 (single
+    // N=65,536 / 131,072 models: 836 vs 671 / 1177 vs 1039 G pairs/s; the
+    // batched 4K-131K models: 118 vs 125 ms), four below
+    if (b >= 18) return 0;
     if (b >= 13) return 3;
     return 4;
 }
