@@ -496,7 +496,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                             f2 ax[K], ay[K], az[K], pp[K];
 #pragma unroll
                             for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
-#pragma unroll 2
+#pragma unroll  // whole sub-block: +5% at N=1M over unroll 2
                             for (int u = 0; u < SUBQ; u++) {
                                 const int qd = base + u * Q;
                                 const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);

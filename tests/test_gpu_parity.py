@@ -221,6 +221,31 @@ def test_every_fp64_variant_meets_tolerance(gpu_ctx, star16k, tri16k):
         gpu_ctx.force_variant("fp64", -1)
 
 
+@pytest.mark.parametrize("hp_cluster", [1.0, 0.03])
+def test_dense_near_cluster(gpu_ctx, hp_cluster):
+    """A compact cluster inside a sparse halo: with hp = 1 every cluster pair is
+    a near (FP64) pair, so every near mask of the cluster's warps is full and the
+    warp-cooperative evaluation runs its largest compactions (32 lanes x 16
+    sources per mask); with hp = 0.03 the masks are partly set."""
+    rng = np.random.default_rng(11)
+    nc, nh = 2048, 1000
+    rc = 0.1 * rng.random(nc) ** (1 / 3)
+    rh = 1.0 + 9.0 * rng.random(nh)
+    dirs = rng.normal(size=(nc + nh, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    pos = dirs * np.concatenate([rc, rh])[:, None]
+    m = np.concatenate([rng.uniform(0.5, 1.5, nc), rng.uniform(0.1, 0.2, nh)]) / (nc + nh)
+    hp = np.concatenate([np.full(nc, hp_cluster), np.full(nh, 0.2)])
+    range2 = 4.0 * hp * hp
+    x, y, z = (np.ascontiguousarray(pos[:, d]) for d in range(3))
+    o = oracle.rows(x, y, z, m, range2, 0)
+    for precision, tol in (("fp64", FP64_TOL), ("f32split", F32_TOL)):
+        got = gpu_ctx.forces(x, y, z, m, range2, 0, precision)
+        r = err_report(*got, *o)
+        print(precision, hp_cluster, r)
+        assert r["acc_max"] <= tol and r["pot_max"] <= tol, (precision, r)
+
+
 def test_red_giant_core_subset(gpu_ctx):
     """Config-3 physics (core point mass, h and m spanning decades) at
     N=65,536 on a row subset: split-FP32 within 1e-6 of the FP64 oracle."""
