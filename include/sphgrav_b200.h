@@ -15,13 +15,14 @@
  *
  * Precisions:
  *   SPHGRAV_FP64       plain FP64 kernel; matches the CPU path to ~1e-12.
- *   SPHGRAV_F32SPLIT   positions as FP32 hi+lo pairs, pair sums in FP32 with one
- *                      Newton step per rsqrt and compensated (Kahan/TwoSum)
- *                      partial sums; FP64 for the split, the cross-block
- *                      partial sums, the near-field (r < max H) pairs and the
- *                      potential-energy diagnostic.  Max relative error of the
- *                      acceleration is ~1e-6 or better for well-conditioned
- *                      particles.
+ *   SPHGRAV_F32SPLIT   positions as FP32 hi+lo pairs; pair terms in FP32 with
+ *                      rsqrt.approx (variants named *_newton add one Newton
+ *                      step) summed into compensated (Kahan/TwoSum) partial
+ *                      sums; FP64 for the split, the cross-block partial sums,
+ *                      the pairs with r < band * max H (band 2 by default,
+ *                      sphgrav_set_fp64_band) and the potential-energy
+ *                      diagnostic.  Max relative error of the acceleration is
+ *                      ~1e-6 or better for well-conditioned particles.
  *
  * Threading: a context is used by one host thread at a time.  Calls enqueue
  * work on the context's stream; functions that return results to host

@@ -270,7 +270,11 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     // defaults by pair-weighted mean N (measured on B200): two rows per
     // thread from 2^18 on, two threads per row for 2^13..2^18 (single
     // N=65,536 / 131,072 models: 836 vs 671 / 1177 vs 1039 G pairs/s; the
-    // batched 4K-131K models: 118 vs 125 ms), four below
+    // batched 4K-131K models: 118 vs 125 ms), four below.  All without the
+    // Newton step on rsqrt.approx: in FP32 the step's own roundings cost
+    // more than it corrects (RMS error 3.2e-8 vs 3.7e-8 at N=1M, 2.7e-8 vs
+    // 4.4e-8 at N=16K, max error equal or lower on every workload) and it
+    // is 3 of 16 FMA-pipe lane-ops per pair (+15% pairs/s at N=1M).
     if (b >= 18) return 0;
     if (b >= 13) return 3;
     return 4;
@@ -997,7 +1001,7 @@ int sphgrav_autotune(sphgrav_ctx *c, int nsets, const int *offsets, const double
     int best = -1;
     for (int v = 0; v < variant_count(precision); v++) {
         const VariantInfo &V = variant_info(precision, v);
-        if (precision == SPHGRAV_F32SPLIT && !V.newton) continue;  // keeps the precision contract
+        if (precision == SPHGRAV_F32SPLIT && V.newton) continue;  // same numerics as the defaults
         c->forced_variant[precision] = v;
         int st = run_device(c, offs, true, 0, 0, in, out, nullptr, nkernel, precision);
         if (st != SPHGRAV_OK) { c->forced_variant[precision] = saved; return st; }

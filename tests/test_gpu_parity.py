@@ -203,8 +203,7 @@ def test_every_f32_variant_meets_tolerance(gpu_ctx, star16k, tri16k):
             got = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
             r = err_report(*got, *tri16k[0])
             print(name, r)
-            tol = F32_TOL if "nonewton" not in name else 4 * F32_TOL
-            assert r["acc_max"] <= tol and r["pot_max"] <= tol, (name, r)
+            assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, (name, r)
     finally:
         gpu_ctx.force_variant("f32split", -1)
 
