@@ -268,7 +268,10 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     }
     if (precision == SPHGRAV_FP64) return 0;
     // defaults by pair-weighted mean N (measured on B200): two rows per
-    // thread from 2^18 on, two threads per row for 2^13..2^18 (single
+    // thread from 2^18 on, with 12 consumer warps (3 per SMSP, as many as the
+    // SMSP that also runs the producer) and a 7-stage ring: 543 vs 560 ms
+    // against 15 warps at N=1M, equal at 262K; two threads per row for
+    // 2^13..2^18 (single
     // N=65,536 / 131,072 models: 836 vs 671 / 1177 vs 1039 G pairs/s; the
     // batched 4K-131K models: 118 vs 125 ms), four below.  All without the
     // Newton step on rsqrt.approx: in FP32 the step's own roundings cost

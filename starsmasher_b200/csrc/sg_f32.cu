@@ -635,14 +635,15 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 }
 
 // name, consumer warps W, rows per thread K, threads per row Q, j-tile TJ, stages NS, Newton step
-#define SG_F32_VARIANTS(X)                                       \
-    X(15, 2, 1, 256, 4, false, "f32split_w15_k2_q1_tj256")        \
-    X(8, 2, 1, 256, 4, false, "f32split_w8_k2_q1_tj256")          \
-    X(15, 1, 1, 256, 4, false, "f32split_w15_k1_q1_tj256")        \
-    X(15, 1, 2, 256, 4, false, "f32split_w15_k1_q2_tj256")        \
-    X(8, 1, 4, 256, 4, false, "f32split_w8_k1_q4_tj256")          \
-    X(15, 2, 1, 256, 4, true, "f32split_w15_k2_q1_tj256_newton")  \
-    X(15, 1, 2, 256, 4, true, "f32split_w15_k1_q2_tj256_newton")  \
+#define SG_F32_VARIANTS(X)                                           \
+    X(12, 2, 1, 256, 7, false, "f32split_w12_k2_q1_tj256_ns7")        \
+    X(15, 2, 1, 256, 4, false, "f32split_w15_k2_q1_tj256")            \
+    X(8, 2, 1, 256, 4, false, "f32split_w8_k2_q1_tj256")              \
+    X(15, 1, 2, 256, 4, false, "f32split_w15_k1_q2_tj256")            \
+    X(8, 1, 4, 256, 4, false, "f32split_w8_k1_q4_tj256")              \
+    X(15, 1, 1, 256, 4, false, "f32split_w15_k1_q1_tj256")            \
+    X(15, 2, 1, 256, 4, true, "f32split_w15_k2_q1_tj256_newton")      \
+    X(15, 1, 2, 256, 4, true, "f32split_w15_k1_q2_tj256_newton")      \
     X(8, 1, 4, 256, 4, true, "f32split_w8_k1_q4_tj256_newton")
 
 #define SG_INFO(W, K, Q, TJ, NS, NW, NAME) {1, (W + 1) * 32, K, Q, TJ, NW ? 1 : 0, NAME, W * 32 * K / Q},
