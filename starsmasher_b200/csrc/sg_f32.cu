@@ -149,6 +149,7 @@ __device__ __noinline__ void near_eval(const SortedF64 D, int nkernel, int jbase
     uint32_t rem = __reduce_or_sync(FULL, wsum);
     int kcur = -1;
     double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+    double2 *res2 = reinterpret_cast<double2 *>(res);  // [32] (a_x, a_y), then [32] (a_z, pot)
     auto fold_row = [&]() {
         if (sx != 0.0 || sy != 0.0 || sz != 0.0 || sp != 0.0) {
             float *acc = s_acc + (kcur * 8) * NT + tid;
@@ -202,19 +203,26 @@ __device__ __noinline__ void near_eval(const SortedF64 D, int nkernel, int jbase
                 const PairOut o = pair_f64_core(D, nkernel, ipo, jbase + j, xj - row[0],
                                                 yj - row[NT], zj - row[2 * NT], rd[j], row[3 * NT],
                                                 rd[TJ + j]);
-                res[lane] = o.ax;
-                res[32 + lane] = o.ay;
-                res[64 + lane] = o.az;
-                res[96 + lane] = o.pot;
+                res2[lane] = make_double2(o.ax, o.ay);
+                res2[32 + lane] = make_double2(o.az, o.pot);
             }
             __syncwarp();
+            // this owner's entries of the round, in order, two at a time into
+            // two partial sums (halves the dependent-add chains)
             const int e1 = min(incl, base + 32);
-            for (int e = max(excl, base); e < e1; e++) {
-                sx += res[e - base];
-                sy += res[32 + e - base];
-                sz += res[64 + e - base];
-                sp += res[96 + e - base];
+            int e = max(excl, base);
+            double tx = 0.0, ty = 0.0, tz = 0.0, tp = 0.0;
+            for (; e + 1 < e1; e += 2) {
+                const double2 a0 = res2[e - base], b0 = res2[32 + e - base];
+                const double2 a1 = res2[e + 1 - base], b1 = res2[33 + e - base];
+                sx += a0.x; sy += a0.y; sz += b0.x; sp += b0.y;
+                tx += a1.x; ty += a1.y; tz += b1.x; tp += b1.y;
             }
+            if (e < e1) {
+                const double2 a0 = res2[e - base], b0 = res2[32 + e - base];
+                sx += a0.x; sy += a0.y; sz += b0.x; sp += b0.y;
+            }
+            sx += tx; sy += ty; sz += tz; sp += tp;
             __syncwarp();
         }
     }
