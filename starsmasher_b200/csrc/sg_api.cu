@@ -267,19 +267,22 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
         if (v >= 0) return v;
     }
     if (precision == SPHGRAV_FP64) return 0;
-    // defaults by pair-weighted mean N (measured on B200): two rows per
-    // thread from 2^18 on, with 12 consumer warps (3 per SMSP, as many as the
-    // SMSP that also runs the producer) and a 7-stage ring: 543 vs 560 ms
-    // against 15 warps at N=1M, equal at 262K; two threads per row for
-    // 2^13..2^18 (single
-    // N=65,536 / 131,072 models: 836 vs 671 / 1177 vs 1039 G pairs/s; the
-    // batched 4K-131K models: 118 vs 125 ms), four below.  All without the
-    // Newton step on rsqrt.approx: in FP32 the step's own roundings cost
-    // more than it corrects (RMS error 3.2e-8 vs 3.7e-8 at N=1M, 2.7e-8 vs
-    // 4.4e-8 at N=16K, max error equal or lower on every workload) and it
-    // is 3 of 16 FMA-pipe lane-ops per pair (+15% pairs/s at N=1M).
-    if (b >= 18) return 0;
-    if (b >= 13) return 3;
+    // defaults by pair-weighted mean N = 2^b, from a sweep of single
+    // polytropes on B200 (G pairs/s of the chosen shape vs the runner-up):
+    //   b >= 20  W12K2Q1, 7 stages   (1M: 2027 vs 1942 for W15K1Q2)
+    //   18..19   W12K1Q1, 7 stages   (262K: 1745 vs 1714; 524K: 1937 vs 1920)
+    //   15..17   W15K1Q2             (32K-131K: 661-1448 vs 548-1410)
+    //   13..14   W12K1Q4, 7 stages   (8K: 178 vs 165; 16K: 370 vs 324)
+    //   <= 12    W8K1Q4              (4K: 75 vs 72)
+    // Twelve consumer warps put the same number of consumers on every SMSP;
+    // all without the Newton step on rsqrt.approx: in FP32 the step's own
+    // roundings cost more than it corrects (RMS error 3.2e-8 vs 3.7e-8 at
+    // N=1M, 2.7e-8 vs 4.4e-8 at N=16K, max error equal or lower on every
+    // workload) and it is 3 of 16 FMA-pipe lane-ops per pair.
+    if (b >= 20) return 0;
+    if (b >= 18) return 2;
+    if (b >= 15) return 3;
+    if (b >= 13) return 5;
     return 4;
 }
 

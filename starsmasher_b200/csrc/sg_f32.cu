@@ -646,10 +646,10 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 #define SG_F32_VARIANTS(X)                                           \
     X(12, 2, 1, 256, 7, false, "f32split_w12_k2_q1_tj256_ns7")        \
     X(15, 2, 1, 256, 4, false, "f32split_w15_k2_q1_tj256")            \
-    X(8, 2, 1, 256, 4, false, "f32split_w8_k2_q1_tj256")              \
+    X(12, 1, 1, 256, 7, false, "f32split_w12_k1_q1_tj256_ns7")        \
     X(15, 1, 2, 256, 4, false, "f32split_w15_k1_q2_tj256")            \
     X(8, 1, 4, 256, 4, false, "f32split_w8_k1_q4_tj256")              \
-    X(15, 1, 1, 256, 4, false, "f32split_w15_k1_q1_tj256")            \
+    X(12, 1, 4, 256, 7, false, "f32split_w12_k1_q4_tj256_ns7")        \
     X(15, 2, 1, 256, 4, true, "f32split_w15_k2_q1_tj256_newton")      \
     X(15, 1, 2, 256, 4, true, "f32split_w15_k1_q2_tj256_newton")      \
     X(8, 1, 4, 256, 4, true, "f32split_w8_k1_q4_tj256_newton")
