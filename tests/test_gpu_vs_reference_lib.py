@@ -1,0 +1,79 @@
+"""The reference's own GPU library against this one, on the benchmark workloads.
+
+oracle/_ref/libsphgrav_ref.so is SPHgrav_lib2 (parallel_bleeding_edge/src/
+SPHgrav_lib2/grav_force_direct.cu: FP32 pair terms on absolute coordinates,
+float-float "ds64" sums) compiled unchanged for sm_100a by oracle/Makefile.
+Both libraries are driven through the same legacy ABI, firsthalf_grav_forces_ /
+lasthalf_grav_forces_ (grav.f:25, balAV3.f:418), from host arrays with every
+copy inside the timed region, and both are scored against this library's FP64
+kernel (<= 1e-12 of the CPU path).  Each case prints one JSON line with the
+pair rates and errors of both.
+"""
+import ctypes
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import err_report
+from starsmasher_b200 import api, inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_lib():
+    if not os.path.exists(oracle.REF_GPU_LIB):
+        pytest.skip("reference GPU library not built (make -C oracle ref)")
+    return ctypes.CDLL(oracle.REF_GPU_LIB, mode=ctypes.RTLD_LOCAL)
+
+
+def _legacy_call(lib, n, arrs, outs, nkernel=0):
+    P = ctypes.POINTER(ctypes.c_double)
+    ia = [ctypes.c_int(v) for v in (n, 1, n, 1, nkernel)]
+    lib.firsthalf_grav_forces_(*(ctypes.byref(v) for v in ia[:3]), *(a.ctypes.data_as(P) for a in arrs),
+                               ctypes.byref(ia[3]), ctypes.byref(ia[4]))
+    rk = ctypes.c_int(0)
+    lib.lasthalf_grav_forces_(ctypes.byref(ia[0]), *(a.ctypes.data_as(P) for a in outs), ctypes.byref(rk))
+
+
+def _best_seconds(fn, reps=2):
+    fn()  # warm-up: allocations, first launch
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
+@pytest.mark.parametrize("workload", ["config2", "config3"])
+def test_faster_and_more_accurate_than_reference_gpu_library(gpu_ctx, workload):
+    ref = _ref_lib()
+    s = inputs.cached(workload)
+    n = s.n
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (s.x, s.y, s.z, s.m, s.range2)]
+    fp64 = gpu_ctx.forces(*arrs, 0, "fp64")
+
+    out_ref = [np.zeros(n) for _ in range(4)]
+    t_ref = _best_seconds(lambda: _legacy_call(ref, n, arrs, out_ref))
+
+    out_our = [np.zeros(n) for _ in range(4)]
+    api.set_legacy_precision("f32split")
+
+    def run_ours():
+        api.firsthalf_grav_forces(n, 1, n, *arrs)
+        api.lasthalf_grav_forces(n, *out_our)
+
+    t_our = _best_seconds(run_ours)
+    r_ref = err_report(*out_ref, *fp64)
+    r_our = err_report(*out_our, *fp64)
+    pairs = float(n) * n
+    print(json.dumps({"workload": workload, "n": n, "path": "legacy ABI, host arrays, copies included",
+                      "reference_gpu_lib": {"gpairs_s": pairs / t_ref / 1e9, "seconds": t_ref, **r_ref},
+                      "this_lib_f32split": {"gpairs_s": pairs / t_our / 1e9, "seconds": t_our, **r_our}}))
+    assert t_our < t_ref
+    assert r_our["acc_max"] <= r_ref["acc_max"]
+    assert r_our["acc_rms"] <= r_ref["acc_rms"]
