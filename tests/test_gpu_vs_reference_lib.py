@@ -77,3 +77,42 @@ def test_faster_and_more_accurate_than_reference_gpu_library(gpu_ctx, workload):
     assert t_our < t_ref
     assert r_our["acc_max"] <= r_ref["acc_max"]
     assert r_our["acc_rms"] <= r_ref["acc_rms"]
+
+
+def test_batched_launch_beats_reference_per_set_calls(gpu_ctx):
+    """Config 4 (64 models, N log-uniform in [4,096, 131,072]).  The reference
+    library has no batch entry point, so its way to evaluate the models is one
+    firsthalf/lasthalf call per model; this library evaluates all of them in
+    one persistent launch (sphgrav_batch_forces, host arrays in and out)."""
+    ref = _ref_lib()
+    b = inputs.cached("config4")
+    offs = [int(v) for v in b.offsets]
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (b.x, b.y, b.z, b.m, b.range2)]
+    subsets = [[a[offs[s]:offs[s + 1]].copy() for a in arrs] for s in range(b.nsets)]
+    out_ref = [[np.zeros(offs[s + 1] - offs[s]) for _ in range(4)] for s in range(b.nsets)]
+
+    def run_ref():
+        for s in range(b.nsets):
+            _legacy_call(ref, offs[s + 1] - offs[s], subsets[s], out_ref[s])
+
+    t_ref = _best_seconds(run_ref)
+    got = {}
+
+    def run_ours():
+        got["r"] = gpu_ctx.batch_forces(offs, *arrs, 0, "f32split")
+
+    t_our = _best_seconds(run_ours)
+    fp64 = [np.zeros(b.n) for _ in range(4)]
+    for s in range(b.nsets):
+        o = gpu_ctx.forces(*subsets[s], 0, "fp64")
+        for c in range(4):
+            fp64[c][offs[s]:offs[s + 1]] = o[c]
+    r_ref = err_report(*(np.concatenate([out_ref[s][c] for s in range(b.nsets)]) for c in range(4)), *fp64)
+    r_our = err_report(*got["r"][:4], *fp64)
+    pairs = float(b.pairs)
+    print(json.dumps({"workload": "config4", "nsets": b.nsets, "n": b.n,
+                      "path": "reference: 64 legacy-ABI calls; this lib: one sphgrav_batch_forces; host arrays",
+                      "reference_gpu_lib": {"gpairs_s": pairs / t_ref / 1e9, "seconds": t_ref, **r_ref},
+                      "this_lib_batched": {"gpairs_s": pairs / t_our / 1e9, "seconds": t_our, **r_our}}))
+    assert t_our < t_ref
+    assert r_our["acc_max"] <= r_ref["acc_max"]
