@@ -167,10 +167,17 @@ int sphgrav_kick_reset(sphgrav_ctx *ctx, unsigned long long c);
 /* Capture the context's work between begin and end into a CUDA graph.
  * Inside the capture only *_device entry points may be called, and each of
  * them must have been called once before with the same sizes, so that every
- * buffer already exists. */
+ * buffer already exists.  The graph bakes in the context's work plan and
+ * buffer addresses: after any later call on the context that changes them
+ * (other sizes, precision or variant) or after sphgrav_destroy,
+ * sphgrav_graph_launch refuses with SPHGRAV_ERR_PROTOCOL and the graph must
+ * be captured again.  Calls with the captured sizes may interleave with
+ * replays. */
 int sphgrav_capture_begin(sphgrav_ctx *ctx);
 int sphgrav_capture_end(sphgrav_ctx *ctx, sphgrav_graph **graph);
 int sphgrav_graph_launch(sphgrav_graph *graph, int repeats);
+/* 1 while the graph may be replayed (see above), else 0. */
+int sphgrav_graph_valid(const sphgrav_graph *graph);
 int sphgrav_graph_destroy(sphgrav_graph *graph);
 
 /* ------------------------------------------------------------ tuning --- */

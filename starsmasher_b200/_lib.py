@@ -51,6 +51,7 @@ SIGNATURES = {
     "sphgrav_capture_begin": (_I, [_P]),
     "sphgrav_capture_end": (_I, [_P, ctypes.POINTER(_P)]),
     "sphgrav_graph_launch": (_I, [_P, _I]),
+    "sphgrav_graph_valid": (_I, [_P]),
     "sphgrav_graph_destroy": (_I, [_P]),
     "sphgrav_autotune": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _I]),
     "sphgrav_tuning_save": (_I, [_P, ctypes.c_char_p]),

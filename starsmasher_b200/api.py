@@ -63,6 +63,12 @@ class Graph:
     def launch(self, repeats: int = 1) -> None:
         check(load().sphgrav_graph_launch(self._h, int(repeats)), "sphgrav_graph_launch")
 
+    @property
+    def valid(self) -> bool:
+        """False once a call on its context changed the work plan or buffers
+        (other sizes, precision or variant) or the context was destroyed."""
+        return bool(self._h) and bool(load().sphgrav_graph_valid(self._h))
+
     def close(self) -> None:
         if self._h:
             load().sphgrav_graph_destroy(self._h)

@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <set>
 #include <string>
 #include <vector>
 #include "sg_launch.h"
@@ -137,11 +138,16 @@ struct Plan {
     std::vector<WorkItem> items;
 };
 
+// A captured graph bakes in the context's work plan and buffer addresses.
+// The context counts every change of either (`epoch`); a graph replays only
+// while the count is the one it was captured at and the context is alive.
 struct sphgrav_graph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;
     int device = 0;
+    sphgrav_ctx *ctx = nullptr;  // null once the context is destroyed
+    unsigned long long epoch = 0;
 };
 
 struct sphgrav_ctx {
@@ -150,6 +156,8 @@ struct sphgrav_ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     bool capturing = false;
+    unsigned long long epoch = 1;       // bumped by every plan rebuild and buffer reallocation
+    std::set<sphgrav_graph *> graphs;   // live graphs captured from this context
 
     DBuf<double> in;    // 5 * cap: x y z m range2 (caller order)
     DBuf<double> out;   // 4 * cap: ax ay az pot (caller order)
@@ -201,6 +209,7 @@ static int ensure(sphgrav_ctx *c, DBuf<T> &b, size_t n, const char *what)
                        what, n);
     size_t want = std::max<size_t>(n, (size_t)(b.cap * 1.25));
     if (want == 0) want = 1;
+    ++c->epoch;
     b.release();
     CUDA_TRY(cudaMalloc((void **)&b.p, want * sizeof(T)));
     b.cap = want;
@@ -212,6 +221,7 @@ static int ensure_pinned(sphgrav_ctx *c, PinnedBuf &b, size_t bytes)
     if (bytes <= b.cap && b.p) return SPHGRAV_OK;
     if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "host staging cannot grow during capture");
     size_t want = std::max<size_t>(bytes, (size_t)(b.cap * 1.25));
+    ++c->epoch;
     b.release();
     CUDA_TRY(cudaMallocHost(&b.p, want));
     b.cap = want;
@@ -412,6 +422,7 @@ static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_ro
                            "with the same sizes before capturing");
         Plan P;
         TRY(build_plan(c, offsets, full_rows, i_lo, ni, precision, variant, P));
+        ++c->epoch;  // graphs captured under the old plan must not replay
         TRY(ensure(c, c->sets, std::max(1, P.nsets), "sets"));
         TRY(ensure(c, c->tile_set, std::max(1, P.ntiles), "tile_set"));
         TRY(ensure(c, c->meta_set, std::max(1, P.nmeta), "meta_set"));
@@ -712,6 +723,8 @@ int sphgrav_destroy(sphgrav_ctx *c)
     if (cur != c->device) cudaSetDevice(c->device);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
+    for (sphgrav_graph *G : c->graphs) G->ctx = nullptr;  // they refuse to launch from now on
+    c->graphs.clear();
     c->in.release(); c->out.release(); c->keys_in.release(); c->keys_out.release();
     c->bbox.release(); c->vals_in.release(); c->vals_out.release(); c->ilist.release();
     c->nsel.release(); c->tile_set.release(); c->meta_set.release(); c->head.release();
@@ -946,19 +959,32 @@ int sphgrav_capture_end(sphgrav_ctx *c, sphgrav_graph **out)
     G->graph = g;
     G->stream = c->stream;
     G->device = c->device;
+    G->ctx = c;
+    G->epoch = c->epoch;
     cudaError_t e = cudaGraphInstantiate(&G->exec, g, 0);
     if (e != cudaSuccess) {
         cudaGraphDestroy(g);
         delete G;
         return set_err(SPHGRAV_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
     }
+    c->graphs.insert(G);
     *out = G;
     return SPHGRAV_OK;
+}
+
+int sphgrav_graph_valid(const sphgrav_graph *G)
+{
+    return G && G->ctx && G->ctx->epoch == G->epoch ? 1 : 0;
 }
 
 int sphgrav_graph_launch(sphgrav_graph *G, int repeats)
 {
     if (!G || repeats < 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad graph launch");
+    if (!G->ctx) return set_err(SPHGRAV_ERR_PROTOCOL, "the graph's context was destroyed");
+    if (G->ctx->epoch != G->epoch)
+        return set_err(SPHGRAV_ERR_PROTOCOL,
+                       "the context's work plan or buffers changed after this graph was captured "
+                       "(a call with other sizes, precision or variant); capture it again");
     for (int r = 0; r < repeats; r++) {
         CUDA_TRY(cudaGraphLaunch(G->exec, G->stream));
         ++g_launches;
@@ -969,6 +995,7 @@ int sphgrav_graph_launch(sphgrav_graph *G, int repeats)
 int sphgrav_graph_destroy(sphgrav_graph *G)
 {
     if (!G) return SPHGRAV_OK;
+    if (G->ctx) G->ctx->graphs.erase(G);
     if (G->exec) cudaGraphExecDestroy(G->exec);
     if (G->graph) cudaGraphDestroy(G->graph);
     delete G;

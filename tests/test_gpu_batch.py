@@ -149,6 +149,49 @@ def test_capture_refuses_new_sizes(gpu_ctx):
     gpu_ctx.sync()
 
 
+def test_graph_refuses_replay_after_plan_change():
+    """A graph bakes in its context's work plan and buffer addresses.  Calls
+    with the captured sizes may interleave with replays; once a call with
+    another precision rebuilds the plan, or the context is destroyed, the
+    graph reports itself invalid and sphgrav_graph_launch refuses.  Validity
+    is asserted before every launch, so no stale graph is ever replayed."""
+    from starsmasher_b200 import Context, _lib
+    t = _t()
+    b = inputs.batch_models(3, 500, 1500, seed=71)
+    X = [dev(a) for a in (b.x, b.y, b.z, b.m, b.range2)]
+    outs = [t.zeros(b.n, dtype=t.float64, device="cuda") for _ in range(4)]
+    ctx = Context(0)  # its own context: the shared fixture's plan stays as it is
+    try:
+        ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")
+        with ctx.capture() as cap:
+            ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")
+        g = cap.graph
+        assert g.valid
+        g.launch(1)
+        ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")  # same plan
+        assert g.valid
+        g.launch(1)
+        ctx.sync()
+        ctx.batch_forces_device(b.offsets, *X, *outs, precision="fp64")  # plan rebuilt
+        ctx.sync()
+        assert not g.valid
+        with pytest.raises(_lib.SphgravError) as e:
+            g.launch(1)
+        assert e.value.status == _lib.ERR_PROTOCOL
+        g.close()
+        with ctx.capture() as cap:
+            ctx.batch_forces_device(b.offsets, *X, *outs, precision="fp64")
+        g2 = cap.graph
+        assert g2.valid
+    finally:
+        ctx.close()
+    assert not g2.valid  # context destroyed
+    with pytest.raises(_lib.SphgravError) as e:
+        g2.launch(1)
+    assert e.value.status == _lib.ERR_PROTOCOL
+    g2.close()
+
+
 def test_autotune_and_cache_file(gpu_ctx, tmp_path):
     b = inputs.batch_models(4, 2000, 4000, seed=61)
     X = [dev(a) for a in (b.x, b.y, b.z, b.m, b.range2)]
