@@ -68,6 +68,26 @@ def test_batch_equals_separate_calls(gpu_ctx, small_batch, precision):
         np.testing.assert_allclose(pot[a:e], g[3], rtol=tol)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "f32split"])
+def test_empty_inputs_and_empty_sets(gpu_ctx, precision):
+    """N = 0 returns empty results; empty sets inside a batch get no rows and
+    W = 0, and leave the other sets' results as separate calls give them."""
+    e = np.zeros(0)
+    got = gpu_ctx.forces(e, e, e, e, e, 0, precision)
+    assert all(a.shape == (0,) for a in got)
+    b = inputs.batch_models(2, 300, 700, seed=53)
+    n0 = int(b.offsets[1])
+    offs = [0, 0, n0, n0, b.n, b.n]  # sets 0, 2 and 4 are empty
+    res = gpu_ctx.batch_forces(offs, b.x, b.y, b.z, b.m, b.range2, 0, precision)
+    W = res[4]
+    assert W[0] == 0.0 and W[2] == 0.0 and W[4] == 0.0
+    for s, (a, c) in enumerate([(0, n0), (n0, b.n)]):
+        one = gpu_ctx.forces(b.x[a:c], b.y[a:c], b.z[a:c], b.m[a:c], b.range2[a:c], 0, precision)
+        for u, v in zip(res[:4], one):
+            assert np.array_equal(u[a:c], v)
+        assert W[2 * s + 1] == pytest.approx(0.5 * np.sum(b.m[a:c] * one[3]), rel=1e-12)
+
+
 def test_batch_device_api_and_W(gpu_ctx, small_batch, small_batch_oracle):
     t = _t()
     b = small_batch
