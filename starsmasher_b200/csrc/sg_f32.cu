@@ -19,14 +19,16 @@
 // (set, i-tile, j-chunk) items):
 //   * one producer warp: issues 1-D bulk async copies (cp.async.bulk, the
 //     TMA engine; no multicast) of each j-tile's SoA arrays x_hi, x_lo, y_hi,
-//     y_lo, z_hi, z_lo, m, H^2 and bounding-box records into a double-
-//     buffered raw area, waits for their mbarrier transaction count, rewrites
-//     the tile as i-tile-relative floats into an NS-stage ring and signals
-//     the stage "full";
+//     y_lo, z_hi, z_lo, m, H^2, FP64 m and H^2, and bounding-box records into
+//     an NS-stage raw ring, waits for their mbarrier transaction count,
+//     rewrites the tile as i-tile-relative floats into the stage's computed
+//     part and signals the stage "full";
 //   * W consumer warps: each owns 32*K/Q rows in registers, waits for a full
 //     stage, sums the tile, and signals it "empty".  Consumers never meet at
 //     a CTA-wide barrier inside an item, so warps that hit near-field pairs
-//     may run behind the others by up to NS-1 tiles.
+//     may run behind the others by up to NS-1 tiles.  W = 12 puts three
+//     consumer warps on every SMSP; with W = 15 the producer's SMSP has one
+//     fewer, and its warps finish tiles early and wait on the ring.
 //   * every mbarrier wait is a bounded poll; a timeout sets an error bit and
 //     the CTA leaves at the next item boundary after its copies have landed.
 //
@@ -35,15 +37,17 @@
 //     staged sources are re-expressed relative to the i-tile's centre c:
 //     x' = (x_hi - c_hi) + (x_lo - c_lo), a few flops per staged particle
 //     instead of per pair.
-//   * sums run in FP32 over sub-blocks of 8 sources per lane, are added into
-//     a per-tile FP32 sum that folds into compensated (TwoSum, "Kahan") float
-//     hi/lo accumulators in shared memory once per tile.
-//   * pairs with r < 2 max(H_i, H_j) are evaluated in FP64 (pair_f64_slots,
-//     the CPU-path formulas) after the tile's FP32 loop and folded into the
-//     same accumulators: below H the softened near field, whose reference
-//     polynomials cancel by up to ~1e3 near q = 1, and between H and 2H the
-//     largest Newtonian terms (see ComputeArgs::band2).  A warp skips the per-pair
-//     test for a tile when the bounding boxes of its rows and of the tile are
+//   * sums run in FP32 over sub-blocks (8 terms per accumulator lane), are
+//     added into a per-tile FP32 sum that folds into compensated (TwoSum,
+//     "Kahan") float hi/lo accumulators in shared memory once per tile.
+//   * pairs with r < 2 max(H_i, H_j) are masked out of the FP32 sums by the
+//     checked loop, flagged in per-thread bit masks, and evaluated after the
+//     tile's FP32 loop in FP64 with the CPU-path formulas, one pair per lane
+//     of the warp (near_eval), then folded into the same accumulators: below
+//     H the softened near field, whose reference polynomials cancel by up to
+//     ~1e3 near q = 1, and between H and 2H the largest Newtonian terms (see
+//     ComputeArgs::band2).  A warp skips the per-pair test (the far loop)
+//     for a tile when the bounding boxes of its rows and of the tile are
 //     farther apart than 2 max(H) of both.
 //   * per (row, j-chunk) results leave the CTA as FP64 partial sums merged in
 //     chunk order (k_merge).
