@@ -19,6 +19,7 @@
 #include <map>
 #include <set>
 #include <string>
+#include <thread>
 #include <vector>
 #include "sg_launch.h"
 #include "../../include/sphgrav_b200.h"
@@ -582,18 +583,76 @@ static int read_device_error(sphgrav_ctx *c)
 
 // Host-side check of the inputs, the reference's asserts
 // (grav_force_direct.cu:601-602) as a status.
+static bool particle_ok(int i, const double *const a[5])
+{
+    const double m = a[3][i], r2 = a[4][i];
+    return m > 0.0 && std::isfinite(m) && r2 != 0.0 && std::isfinite(r2) && std::isfinite(a[0][i]) &&
+           std::isfinite(a[1][i]) && std::isfinite(a[2][i]);
+}
+
+static int report_bad_particle(int i, const double *const a[5])
+{
+    const double m = a[3][i], r2 = a[4][i];
+    if (!(m > 0.0) || !std::isfinite(m))
+        return set_err(SPHGRAV_ERR_INVALID_INPUT, "mass[%d] = %g must be > 0", i, m);
+    if (r2 == 0.0 || !std::isfinite(r2))
+        return set_err(SPHGRAV_ERR_INVALID_INPUT, "range2[%d] = %g must be non-zero", i, r2);
+    return set_err(SPHGRAV_ERR_INVALID_INPUT, "position of particle %d is not finite", i);
+}
+
+// Host passes over the caller's (pageable) arrays -- copies into and out of
+// the pinned staging buffers, input validation -- run on up to 8 threads
+// once they are a few MB: a single thread moves ~5-10 GB/s, which at
+// N = 1M made the staging a few percent of a host-array call.
+static int host_threads(size_t bytes)
+{
+    if (bytes < ((size_t)4 << 20)) return 1;
+    const unsigned hc = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(hc ? hc : 1u, 8u));
+}
+
+// f(i0, i1, t) over nt contiguous ranges of [0, n); ranges that get no
+// thread (thread creation failed) run on the calling thread.
+template <class F>
+static void parallel_ranges(int n, int nt, const F &f)
+{
+    auto lo = [&](int t) { return (int)((long long)n * t / nt); };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) {
+        try {
+            th.emplace_back(f, lo(t), lo(t + 1), t);
+        } catch (...) {
+            break;
+        }
+    }
+    for (int t = (int)th.size() + 1; t < nt; t++) f(lo(t), lo(t + 1), t);
+    f(0, lo(1), 0);
+    for (auto &x : th) x.join();
+}
+
 static int check_host_inputs(int n, const double *x, const double *y, const double *z,
                              const double *m, const double *r2)
 {
-    for (int i = 0; i < n; i++) {
-        if (!(m[i] > 0.0) || !std::isfinite(m[i]))
-            return set_err(SPHGRAV_ERR_INVALID_INPUT, "mass[%d] = %g must be > 0", i, m[i]);
-        if (r2[i] == 0.0 || !std::isfinite(r2[i]))
-            return set_err(SPHGRAV_ERR_INVALID_INPUT, "range2[%d] = %g must be non-zero", i, r2[i]);
-        if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i]))
-            return set_err(SPHGRAV_ERR_INVALID_INPUT, "position of particle %d is not finite", i);
-    }
-    return SPHGRAV_OK;
+    const double *a[5] = {x, y, z, m, r2};
+    const int nt = host_threads(5 * sizeof(double) * (size_t)n);
+    std::vector<int> first(nt, n);
+    parallel_ranges(n, nt, [&](int i0, int i1, int t) {
+        for (int i = i0; i < i1; i++)
+            if (!particle_ok(i, a)) { first[t] = i; break; }
+    });
+    const int bad = *std::min_element(first.begin(), first.end());
+    return bad < n ? report_bad_particle(bad, a) : SPHGRAV_OK;
+}
+
+// Copy count arrays of n doubles (src[q] + off) to dst[q] + doff, in parallel
+// slices of the index range.
+static void copy_arrays(int count, int n, double *const *dst, size_t doff, const double *const *src,
+                        size_t soff)
+{
+    parallel_ranges(n, host_threads(count * sizeof(double) * (size_t)n), [&](int i0, int i1, int) {
+        for (int q = 0; q < count; q++)
+            memcpy(dst[q] + doff + i0, src[q] + soff + i0, sizeof(double) * (size_t)(i1 - i0));
+    });
 }
 
 // Context-owned input (5 arrays) and output (4 arrays) buffers of io_cap
@@ -617,7 +676,9 @@ static int upload_inputs(sphgrav_ctx *c, int n, const double *x, const double *y
     TRY(ensure_pinned(c, c->h_in, 5 * sizeof(double) * std::max(n, 1)));
     double *h = (double *)c->h_in.p;
     const double *src[5] = {x, y, z, m, r2};
-    for (int a = 0; a < 5; a++) memcpy(h + (size_t)a * n, src[a], sizeof(double) * n);
+    double *dst[5];
+    for (int a = 0; a < 5; a++) dst[a] = h + (size_t)a * n;
+    copy_arrays(5, n, dst, 0, src, 0);
     const size_t cap = c->io_cap;
     if (n > 0) {
         // the device buffer holds 5 arrays of io_cap; copy each
@@ -833,7 +894,8 @@ int sphgrav_batch_forces(sphgrav_ctx *c, int nsets, const int *offsets, const do
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     TRY(read_device_error(c));
     double *dst[4] = {ax, ay, az, pot};
-    for (int q = 0; q < 4; q++) memcpy(dst[q], h + (size_t)q * n, sizeof(double) * n);
+    const double *src[4] = {h, h + (size_t)n, h + 2 * (size_t)n, h + 3 * (size_t)n};
+    copy_arrays(4, n, dst, 0, src, 0);
     if (W_per_set) memcpy(W_per_set, h + 4 * (size_t)n, sizeof(double) * nsets);
     return SPHGRAV_OK;
 }
@@ -890,7 +952,8 @@ int sphgrav_lasthalf(sphgrav_ctx *c, double *ax, double *ay, double *az, double 
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL output pointer");
     const double *h = (const double *)c->h_out.p;
     double *dst[4] = {ax, ay, az, pot};
-    for (int q = 0; q < 4; q++) memcpy(dst[q] + i0, h + (size_t)q * ni, sizeof(double) * ni);
+    const double *src[4] = {h, h + (size_t)ni, h + 2 * (size_t)ni, h + 3 * (size_t)ni};
+    copy_arrays(4, ni, dst, (size_t)i0, src, 0);
     return SPHGRAV_OK;
 }
 
