@@ -116,6 +116,17 @@ int sphgrav_lasthalf(sphgrav_ctx *ctx, double *ax, double *ay, double *az,
  * [ngrav_lower, ngrav_upper] (1-based, inclusive, as main.f:283-295 sets
  * them); lasthalf (balAV3.f:418) then fills gx, gy, gz, grpot at those rows.
  * Host arrays of length ntot.  Blocking. */
+/* Device-resident form of sphgrav_gravforce: x, y, z, am, hp, u and the
+ * outputs are device arrays of length ntot.  range2 (grav.f:15-18) is built
+ * on the device into a context buffer, and rows [ngrav_lower, ngrav_upper]
+ * (1-based, inclusive) of gx, gy, gz, grpot are written; the other rows are
+ * left as they are.  Asynchronous on the context's stream, like
+ * sphgrav_forces_device, and capturable once called with the same sizes. */
+int sphgrav_gravforce_device(sphgrav_ctx *ctx, int ntot, int ngrav_lower, int ngrav_upper,
+                             const double *x, const double *y, const double *z,
+                             const double *am, const double *hp, const double *u,
+                             int nkernel, int precision, double *gx, double *gy,
+                             double *gz, double *grpot);
 int sphgrav_gravforce(sphgrav_ctx *ctx, int ntot, int ngrav_lower, int ngrav_upper,
                       const double *x, const double *y, const double *z,
                       const double *am, const double *hp, const double *u,

@@ -46,6 +46,7 @@ SIGNATURES = {
     "sphgrav_batch_forces_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P]),
     "sphgrav_batch_forces": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P]),
     "sphgrav_gravforce": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
+    "sphgrav_gravforce_device": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
     "sphgrav_kick_positions_device": (_I, [_P, _I, _P, _P, _P, _D, ctypes.c_ulonglong]),
     "sphgrav_kick_reset": (_I, [_P, ctypes.c_ulonglong]),
     "sphgrav_capture_begin": (_I, [_P]),

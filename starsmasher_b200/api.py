@@ -170,6 +170,18 @@ class Context:
               "sphgrav_gravforce")
         return tuple(outs)
 
+    def gravforce_device(self, ntot: int, x, y, z, am, hp, u, gx, gy, gz, grpot,
+                         ngrav_lower: int = 1, ngrav_upper: Optional[int] = None,
+                         nkernel: int = 0, precision="f32split") -> None:
+        """Device-resident gravforce: range2 built on the device, rows
+        [ngrav_lower, ngrav_upper] (1-based) of gx, gy, gz, grpot written."""
+        ngrav_upper = ntot if ngrav_upper is None else ngrav_upper
+        check(self._lib.sphgrav_gravforce_device(self._h, int(ntot), int(ngrav_lower), int(ngrav_upper),
+                                                 _dp(x), _dp(y), _dp(z), _dp(am), _dp(hp), _dp(u),
+                                                 int(nkernel), _prec(precision), _dp(gx), _dp(gy),
+                                                 _dp(gz), _dp(grpot)),
+              "sphgrav_gravforce_device")
+
     def batch_forces(self, offsets: Sequence[int], x, y, z, mass, range2, nkernel: int = 0,
                      precision="f32split"):
         offs = np.ascontiguousarray(offsets, dtype=np.int32)

@@ -177,6 +177,7 @@ struct sphgrav_ctx {
     DBuf<WorkItem> items;
     DBuf<double> partials, wtile, wdev;
     DBuf<unsigned long long> kick_counter;
+    DBuf<double> range2;  // sphgrav_gravforce_device: range2 built on the device
     DBuf<float> probe_sink;
 
     PinnedBuf h_in, h_out, h_err;
@@ -793,6 +794,7 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->orig.release(); c->flag.release(); c->f32.release(); c->sets.release();
     c->imeta.release(); c->jmeta.release(); c->items.release(); c->partials.release();
     c->wtile.release(); c->wdev.release(); c->kick_counter.release(); c->probe_sink.release();
+    c->range2.release();
     c->h_in.release(); c->h_out.release(); c->h_err.release();
     for (auto &e : c->prof_events) {
         cudaEventDestroy(e.first);
@@ -976,6 +978,24 @@ int sphgrav_gravforce(sphgrav_ctx *c, int ntot, int ngrav_lower, int ngrav_upper
     TRY(sphgrav_firsthalf(c, ntot, ngrav_lower - 1, len, x, y, z, am, range2.data(), nkernel,
                           precision));
     return sphgrav_lasthalf(c, gx, gy, gz, grpot);
+}
+
+int sphgrav_gravforce_device(sphgrav_ctx *c, int ntot, int ngrav_lower, int ngrav_upper,
+                             const double *x, const double *y, const double *z, const double *am,
+                             const double *hp, const double *u, int nkernel, int precision,
+                             double *gx, double *gy, double *gz, double *grpot)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (ntot < 0 || ngrav_lower < 1 || ngrav_upper < ngrav_lower - 1 || ngrav_upper > ntot)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad row range [%d, %d] of %d", ngrav_lower,
+                       ngrav_upper, ntot);
+    if (ntot > 0 && (!hp || !u)) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL hp or u");
+    TRY(use_device(c));
+    TRY(ensure(c, c->range2, std::max(ntot, 1), "range2"));
+    CUDA_TRY(launch_range2(ntot, hp, u, c->range2.p, c->stream));  // grav.f:15-18
+    const int len = ngrav_upper - ngrav_lower + 1;                   // grav.f:23
+    return sphgrav_forces_device(c, ntot, ngrav_lower - 1, len, x, y, z, am, c->range2.p, nkernel,
+                                 precision, gx, gy, gz, grpot, nullptr);
 }
 
 // ------------------------------------------------------ sweeps & capture

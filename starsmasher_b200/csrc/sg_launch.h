@@ -85,6 +85,7 @@ cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, int ntiles_to
                          OutputsDev out, double *wtile, cudaStream_t st);
 cudaError_t launch_wsum(const SetDesc *sets, int nsets, const double *wtile, double *W,
                         cudaStream_t st);
+cudaError_t launch_range2(int n, const double *hp, const double *u, double *range2, cudaStream_t st);
 cudaError_t launch_kick(int n, double *x, double *y, double *z, double sigma,
                         unsigned long long seed, unsigned long long *counter, cudaStream_t st);
 cudaError_t launch_fp32_probe(int iters, int blocks, float *sink, cudaStream_t st);

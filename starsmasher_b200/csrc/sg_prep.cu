@@ -502,6 +502,24 @@ __global__ void k_kick(int n, double *x, double *y, double *z, double sigma,
 }
 __global__ void k_kick_advance(unsigned long long *counter) { *counter += 1; }
 
+// ------------------------------------------- Fortran caller's range2 (grav.f:15-18)
+// range2 = 4 hp^2, negated for point masses (u == 0)
+__global__ void k_range2(int n, const double *hp, const double *u, double *range2)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double r = 4.0 * hp[i] * hp[i];
+        range2[i] = u[i] == 0.0 ? -r : r;
+    }
+}
+
+cudaError_t launch_range2(int n, const double *hp, const double *u, double *range2, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    k_range2<<<grid_for(n, 256, 4096), 256, 0, st>>>(n, hp, u, range2);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_kick(int n, double *x, double *y, double *z, double sigma,
                         unsigned long long seed, unsigned long long *counter, cudaStream_t st)
 {

@@ -53,6 +53,17 @@ module sphgrav_b200_mod
       real(c_double), intent(inout) :: gx(*), gy(*), gz(*), grpot(*)
     end function
 
+    ! device-resident form: every array argument is a device pointer (for
+    ! example from OpenACC/CUDA Fortran, or c_loc of a managed array)
+    integer(c_int) function sphgrav_gravforce_device(ctx, ntot, ngrav_lower, ngrav_upper, x, y, z, &
+                                                     am, hp, u, nkernel, precision, gx, gy, gz, &
+                                                     grpot) bind(C, name="sphgrav_gravforce_device")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: ntot, ngrav_lower, ngrav_upper, nkernel, precision
+      type(c_ptr), value :: x, y, z, am, hp, u, gx, gy, gz, grpot
+    end function
+
     integer(c_int) function sphgrav_batch_forces(ctx, nsets, offsets, x, y, z, mass, range2, &
                                                  nkernel, precision, ax, ay, az, pot, w) &
                                                  bind(C, name="sphgrav_batch_forces")

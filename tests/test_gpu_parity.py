@@ -90,6 +90,28 @@ def test_gravforce_host_mirror_matches(gpu_ctx):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "f32split"])
+def test_gravforce_device_matches_host_mirror(gpu_ctx, precision):
+    """sphgrav_gravforce_device (positions, hp, u on the device; range2 built
+    there) gives the host mirror's rows bit for bit and leaves the others."""
+    t = _torch()
+    d = load_golden("3stars_start1")
+    n = d["x"].shape[0]
+    hp = d["hp"]
+    u = d["u"].copy()
+    u[::50] = 0.0  # some point masses: negative range2
+    lo, hi = 11, n - 7
+    want = gpu_ctx.gravforce(d["x"], d["y"], d["z"], d["am"], hp, u, lo, hi, 0, precision)
+    outs = [t.full((n,), -7.0, dtype=t.float64, device="cuda") for _ in range(4)]
+    gpu_ctx.gravforce_device(n, *(dev(a) for a in (d["x"], d["y"], d["z"], d["am"], hp, u)), *outs,
+                             ngrav_lower=lo, ngrav_upper=hi, precision=precision)
+    gpu_ctx.sync()
+    for a, b in zip(outs, want):
+        a = a.cpu().numpy()
+        assert np.array_equal(a[lo - 1:hi], b[lo - 1:hi])
+        assert np.all(a[:lo - 1] == -7.0) and np.all(a[hi:] == -7.0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "f32split"])
 def test_legacy_abi_row_slice(precision, star16k):
     """Fortran conventions: 1-based n_lower, only the listed rows written."""
     s = star16k
