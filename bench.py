@@ -415,7 +415,13 @@ def main():
         v64 = pairs / (ms64 * 1e-3) / 1e9
         res64 = [o.cpu().numpy() for o in outs]
         acc = accuracy(res_f32, res64)
-        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64, "speedup_f32split_vs_fp64": value / world / v64}
+        peak64 = ctx.fp64_peak_probe(100000)
+        ach64 = v64 * 1e9 * FLOPS_PER_PAIR / 1e12
+        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64, "speedup_f32split_vs_fp64": value / world / v64,
+                "roofline": {"bound": "fp64-fma", "achieved": ach64, "peak": peak64, "unit": "TFLOP/s",
+                             "frac": ach64 / peak64, "flops_per_pair": FLOPS_PER_PAIR,
+                             "time": "whole step (preparation included)",
+                             "peak_source": "measured in-run: DFMA throughput probe on this GPU"}}
 
     # ------------------------------------------------------------ roofline
     peak = ctx.fp32_peak_probe(200000)

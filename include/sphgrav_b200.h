@@ -253,6 +253,9 @@ int sphgrav_profile_read(sphgrav_ctx *ctx, double *kernel_ms, int *launches);
  * iterations per thread on the context's device and returns the measured
  * TFLOP/s (2 flops per FMA) in *tflops. */
 int sphgrav_fp32_peak_probe(sphgrav_ctx *ctx, int iters, double *tflops);
+/* FP64 FMA throughput probe: eight independent DFMA chains per thread for
+ * `iters` iterations; the measured TFLOP/s (2 flops per FMA) in *tflops. */
+int sphgrav_fp64_peak_probe(sphgrav_ctx *ctx, int iters, double *tflops);
 
 #ifdef __cplusplus
 }

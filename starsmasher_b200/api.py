@@ -274,6 +274,12 @@ class Context:
               "sphgrav_fp32_peak_probe")
         return t.value
 
+    def fp64_peak_probe(self, iters: int = 20000) -> float:
+        t = ctypes.c_double()
+        check(self._lib.sphgrav_fp64_peak_probe(self._h, int(iters), ctypes.byref(t)),
+              "sphgrav_fp64_peak_probe")
+        return t.value
+
 
 def variant_names(precision) -> list:
     lib = load()

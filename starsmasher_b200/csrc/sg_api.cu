@@ -1247,6 +1247,24 @@ int sphgrav_fp32_peak_probe(sphgrav_ctx *c, int iters, double *tflops)
     return SPHGRAV_OK;
 }
 
+int sphgrav_fp64_peak_probe(sphgrav_ctx *c, int iters, double *tflops)
+{
+    if (!c || !tflops || iters <= 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad probe arguments");
+    TRY(use_device(c));
+    const int blocks = c->sm_count * 8;
+    TRY(ensure(c, c->probe_sink, blocks, "probe"));
+    CUDA_TRY(launch_fp64_probe(std::min(iters, 1000), blocks, c->probe_sink.p, c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev_start, c->stream));
+    CUDA_TRY(launch_fp64_probe(iters, blocks, c->probe_sink.p, c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev_done, c->stream));
+    CUDA_TRY(cudaEventSynchronize(c->ev_done));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, c->ev_start, c->ev_done));
+    const double flops = (double)blocks * 256.0 * iters * 8 * 2;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return SPHGRAV_OK;
+}
+
 // -------------------------------------------------- legacy Fortran ABI
 static sphgrav_ctx *g_legacy = nullptr;
 static int g_legacy_device = -1;

@@ -563,4 +563,29 @@ cudaError_t launch_fp32_probe(int iters, int blocks, float *sink, cudaStream_t s
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------- FP64 FMA probe
+// Eight independent DFMA chains per thread: the FP64 pipe's throughput.
+__global__ void k_fp64_probe(int iters, float *sink)
+{
+    double a[8];
+    const double s = 1.0 + 1e-9 * threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < 8; c++) a[c] = s * (c + 1);
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int c = 0; c < 8; c++) a[c] = fma(a[c], 0.9999999999, 1e-10);
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) acc += a[c];
+    if (acc == 12345.678) sink[blockIdx.x] = (float)acc;
+}
+
+cudaError_t launch_fp64_probe(int iters, int blocks, float *sink, cudaStream_t st)
+{
+    k_fp64_probe<<<blocks, 256, 0, st>>>(iters, sink);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
 }  // namespace sg
