@@ -253,6 +253,13 @@ int sphgrav_profile_read(sphgrav_ctx *ctx, double *kernel_ms, int *launches);
  * iterations per thread on the context's device and returns the measured
  * TFLOP/s (2 flops per FMA) in *tflops. */
 int sphgrav_fp32_peak_probe(sphgrav_ctx *ctx, int iters, double *tflops);
+/* Self-test of the device-side failure path: a one-warp kernel waits, with
+ * the pair kernels' bounded mbarrier poll, on a barrier that nothing arrives
+ * on, gives up after `polls` polls (1..65536) and sets the context's device
+ * error flag as a timed-out pair kernel does.  Returns
+ * SPHGRAV_ERR_DEVICE_TIMEOUT (expected) after clearing the flag; the
+ * context stays usable.  Blocking. */
+int sphgrav_selftest_wait_timeout(sphgrav_ctx *ctx, int polls);
 /* FP64 FMA throughput probe: eight independent DFMA chains per thread for
  * `iters` iterations; the measured TFLOP/s (2 flops per FMA) in *tflops. */
 int sphgrav_fp64_peak_probe(sphgrav_ctx *ctx, int iters, double *tflops);

@@ -67,6 +67,7 @@ SIGNATURES = {
     "sphgrav_last_plan_info": (_I, [_P, _PI, _PI, _PI]),
     "sphgrav_fp32_peak_probe": (_I, [_P, _I, _PD]),
     "sphgrav_fp64_peak_probe": (_I, [_P, _I, _PD]),
+    "sphgrav_selftest_wait_timeout": (_I, [_P, _I]),
     "sphgrav_forces_fp64_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "sphgrav_profile_enable": (_I, [_P, _I]),
     "sphgrav_profile_read": (_I, [_P, _PD, _PI]),

@@ -274,6 +274,11 @@ class Context:
               "sphgrav_fp32_peak_probe")
         return t.value
 
+    def selftest_wait_timeout(self, polls: int = 1024) -> int:
+        """Run the device-timeout self-test; returns its status
+        (ERR_DEVICE_TIMEOUT when the failure path works)."""
+        return int(self._lib.sphgrav_selftest_wait_timeout(self._h, int(polls)))
+
     def fp64_peak_probe(self, iters: int = 20000) -> float:
         t = ctypes.c_double()
         check(self._lib.sphgrav_fp64_peak_probe(self._h, int(iters), ctypes.byref(t)),

@@ -1247,6 +1247,17 @@ int sphgrav_fp32_peak_probe(sphgrav_ctx *c, int iters, double *tflops)
     return SPHGRAV_OK;
 }
 
+int sphgrav_selftest_wait_timeout(sphgrav_ctx *c, int polls)
+{
+    if (!c || polls <= 0 || polls > (1 << 16))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "polls must be in [1, 65536]");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "the self-test cannot be captured");
+    TRY(use_device(c));
+    CUDA_TRY(launch_wait_selftest((uint32_t)polls, c->err.p, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return read_device_error(c);
+}
+
 int sphgrav_fp64_peak_probe(sphgrav_ctx *c, int iters, double *tflops)
 {
     if (!c || !tflops || iters <= 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "bad probe arguments");

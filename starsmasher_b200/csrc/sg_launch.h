@@ -90,5 +90,6 @@ cudaError_t launch_kick(int n, double *x, double *y, double *z, double sigma,
                         unsigned long long seed, unsigned long long *counter, cudaStream_t st);
 cudaError_t launch_fp32_probe(int iters, int blocks, float *sink, cudaStream_t st);
 cudaError_t launch_fp64_probe(int iters, int blocks, float *sink, cudaStream_t st);
+cudaError_t launch_wait_selftest(uint32_t polls, int *err, cudaStream_t st);
 
 }  // namespace sg

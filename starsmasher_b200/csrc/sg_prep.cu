@@ -581,6 +581,26 @@ __global__ void k_fp64_probe(int iters, float *sink)
     if (acc == 12345.678) sink[blockIdx.x] = (float)acc;
 }
 
+// ------------------------------------------- device timeout self-test
+// One warp waits, through the pair kernels' bounded mbarrier poll, on a
+// barrier that nothing arrives on; after `polls` polls it records
+// DEVERR_TIMEOUT the way a pair kernel does and returns.
+__global__ void k_wait_selftest(uint32_t polls, int *err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncwarp();
+    const bool ok = mbar_wait_bounded(&bar, 0, polls);
+    if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicOr(err, DEVERR_TIMEOUT);
+}
+
+cudaError_t launch_wait_selftest(uint32_t polls, int *err, cudaStream_t st)
+{
+    k_wait_selftest<<<1, 32, 0, st>>>(polls, err);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fp64_probe(int iters, int blocks, float *sink, cudaStream_t st)
 {
     k_fp64_probe<<<blocks, 256, 0, st>>>(iters, sink);

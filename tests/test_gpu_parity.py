@@ -207,6 +207,26 @@ def test_protocol_errors(gpu_ctx):
     assert e.value.status == _lib.ERR_INVALID_ARGUMENT
 
 
+def test_device_wait_timeout_is_reported_and_recoverable(gpu_ctx):
+    """The pair kernels' bounded mbarrier wait, run on a barrier that nothing
+    arrives on (sphgrav_selftest_wait_timeout): it gives up after its polls,
+    the host reads SPHGRAV_ERR_DEVICE_TIMEOUT, the flag is cleared and the
+    context keeps working.  No fault and no hang is involved."""
+    import time
+    t0 = time.perf_counter()
+    st = gpu_ctx.selftest_wait_timeout(1024)
+    assert st == _lib.ERR_DEVICE_TIMEOUT
+    assert time.perf_counter() - t0 < 20.0
+    s = inputs.single_polytrope(700, 1.5, seed=5)
+    got = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "fp64")
+    o = oracle.rows(s.x, s.y, s.z, s.m, s.range2, 0)
+    r = err_report(*got, *o)
+    assert r["acc_max"] <= FP64_TOL and r["pot_max"] <= FP64_TOL
+    with pytest.raises(_lib.SphgravError) as e:
+        _lib.check(gpu_ctx._lib.sphgrav_selftest_wait_timeout(gpu_ctx._h, 0), "selftest")
+    assert e.value.status == _lib.ERR_INVALID_ARGUMENT
+
+
 @pytest.mark.parametrize("precision", ["fp64", "f32split"])
 def test_deterministic(gpu_ctx, star16k, precision):
     s = star16k
