@@ -393,9 +393,25 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         sep_ms = e0.elapsed_time(e1) / reps
+        # the same with the plain FP64 kernel: the other reading of "separate
+        # plain launches"
+        def separate_fp64():
+            for s_ in range(ws.nsets):
+                a, b = int(ws.offsets[s_]), int(ws.offsets[s_ + 1])
+                ctx.forces_device(b - a, *(t[a:b] for t in X), *(o[a:b] for o in outs),
+                                  nkernel=args.nkernel, precision="fp64")
+        separate_fp64()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        separate_fp64()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sep64_ms = e0.elapsed_time(e1)
         batch_cmp = {"separate_calls_ms_per_step": sep_ms, "batched_ms_per_step": ms_per_step,
                      "speedup_batched_vs_separate": sep_ms / ms_per_step,
-                     "separate": f"{ws.nsets} sphgrav_forces_device calls, one per set"}
+                     "separate": f"{ws.nsets} sphgrav_forces_device calls, one per set",
+                     "separate_fp64_calls_ms_per_step": sep64_ms,
+                     "speedup_batched_vs_separate_fp64": sep64_ms / ms_per_step}
 
     # --------------------------------------------- FP64 kernel and accuracy
     fp64 = None
