@@ -23,6 +23,13 @@
  *                      sphgrav_set_fp64_band) and the potential-energy
  *                      diagnostic.  Max relative error of the acceleration is
  *                      ~1e-6 or better for well-conditioned particles.
+ *   SPHGRAV_TREE       Barnes-Hut octree, the approximate alternative the
+ *                      reference ships with the same ABI
+ *                      (misc/SPHgravtree_lib): monopole + quadrupole cells,
+ *                      opening angle theta (sphgrav_set_theta, or
+ *                      gpu_init_dev_'s theta for the legacy entry points;
+ *                      default 0.3), softened pairs particle by particle.
+ *                      One particle set per call; not capturable.
  *
  * Threading: a context is used by one host thread at a time.  Calls enqueue
  * work on the context's stream; functions that return results to host
@@ -48,7 +55,7 @@ enum {
     SPHGRAV_ERR_TOO_LARGE = 8          /* size beyond a documented limit */
 };
 
-enum { SPHGRAV_FP64 = 0, SPHGRAV_F32SPLIT = 1 };
+enum { SPHGRAV_FP64 = 0, SPHGRAV_F32SPLIT = 1, SPHGRAV_TREE = 2 };
 
 typedef struct sphgrav_ctx sphgrav_ctx;
 typedef struct sphgrav_graph sphgrav_graph;
@@ -58,7 +65,8 @@ typedef struct sphgrav_graph sphgrav_graph;
  * Fortran passes every argument by reference.  On error these log to stderr
  * and abort, as the reference's assert/exit does (cutil.h:19-27).
  * Precision: SPHGRAV_F32SPLIT unless the environment variable
- * SPHGRAV_PRECISION=fp64 is set (or sphgrav_legacy_set_precision is called).
+ * SPHGRAV_PRECISION=fp64 (or =tree) is set or sphgrav_legacy_set_precision is
+ * called.  gpu_init_dev_'s theta sets the tree mode's opening angle.
  */
 
 /* Replaces firsthalf_grav_forces_ (grav_force_direct.cu:650-656), called from
@@ -208,6 +216,17 @@ int sphgrav_tuning_load(sphgrav_ctx *ctx, const char *path);
  * time in proportion to the pairs it moves (~factor^3 times the near-field
  * pairs).  Factor in [1, 16].  No reference counterpart. */
 int sphgrav_set_fp64_band(sphgrav_ctx *ctx, double factor);
+/* SPHGRAV_TREE: opening angle theta in [0, 2] (default 0.3, the value
+ * main.f:269 passes to gpu_init_dev_).  A node is opened when the gap
+ * between its box and the walking group's box is at most l / theta (l its
+ * edge length) or at most the largest H of either; theta = 0 opens every
+ * node and gives the direct sum. */
+int sphgrav_set_theta(sphgrav_ctx *ctx, double theta);
+/* SPHGRAV_TREE: walking groups of the last tree call and how many of them
+ * were handed to the direct FP64 sum (groups whose particles' softening
+ * spheres hold more than 32,768 particles; their rows are exact direct
+ * sums).  Either pointer may be NULL. */
+int sphgrav_tree_stats(sphgrav_ctx *ctx, int *groups, int *heavy);
 /* Force a kernel variant by index (-1 = automatic) for a precision. */
 int sphgrav_force_variant(sphgrav_ctx *ctx, int precision, int variant);
 /* Number of kernel variants and a printable name of each. */

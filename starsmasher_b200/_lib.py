@@ -23,6 +23,7 @@ ERR_TOO_LARGE = 8
 
 FP64 = 0
 F32SPLIT = 1
+TREE = 2
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -59,6 +60,8 @@ SIGNATURES = {
     "sphgrav_tuning_load": (_I, [_P, ctypes.c_char_p]),
     "sphgrav_force_variant": (_I, [_P, _I, _I]),
     "sphgrav_set_fp64_band": (_I, [_P, _D]),
+    "sphgrav_set_theta": (_I, [_P, _D]),
+    "sphgrav_tree_stats": (_I, [_P, _PI, _PI]),
     "sphgrav_variant_count": (_I, [_I]),
     "sphgrav_variant_name": (ctypes.c_char_p, [_I, _I]),
     "sphgrav_status_string": (ctypes.c_char_p, [_I]),

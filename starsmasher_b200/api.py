@@ -21,9 +21,10 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import F32SPLIT, FP64, check, load
+from ._lib import F32SPLIT, FP64, TREE, check, load
 
-PRECISIONS = {"fp64": FP64, "f32split": F32SPLIT, FP64: FP64, F32SPLIT: F32SPLIT}
+PRECISIONS = {"fp64": FP64, "f32split": F32SPLIT, "tree": TREE, FP64: FP64, F32SPLIT: F32SPLIT,
+              TREE: TREE}
 
 
 def _prec(p) -> int:
@@ -120,6 +121,16 @@ class Context:
     def force_variant(self, precision, variant: int) -> None:
         check(self._lib.sphgrav_force_variant(self._h, _prec(precision), int(variant)),
               "sphgrav_force_variant")
+
+    def set_theta(self, theta: float) -> None:
+        """Tree mode: opening angle (default 0.3; 0 opens every node)."""
+        check(self._lib.sphgrav_set_theta(self._h, float(theta)), "sphgrav_set_theta")
+
+    def tree_stats(self) -> tuple:
+        """Tree mode: (walking groups, groups handed to the direct FP64 sum) of the last call."""
+        g, h = ctypes.c_int(0), ctypes.c_int(0)
+        check(self._lib.sphgrav_tree_stats(self._h, ctypes.byref(g), ctypes.byref(h)), "sphgrav_tree_stats")
+        return g.value, h.value
 
     def set_fp64_band(self, factor: float) -> None:
         """Split-FP32: evaluate pairs with r < factor * max(H) in FP64 (default 2)."""

@@ -178,6 +178,20 @@ struct sphgrav_ctx {
     DBuf<double> partials, wtile, wdev;
     DBuf<unsigned long long> kick_counter;
     DBuf<double> range2;  // sphgrav_gravforce_device: range2 built on the device
+
+    // Barnes-Hut mode (SPHGRAV_TREE)
+    double theta = 0.3;   // opening angle (gpu_init_dev_ passes it; main.f:269)
+    int tree_groups_last = 0, tree_heavy_last = 0;  // walking groups of the last tree call,
+                                                    // and those handed to the direct sum
+    DBuf<TreeNode> tnodes;
+    DBuf<NodeGeom> tgeom;
+    DBuf<NodeMP> tmp;
+    DBuf<int> tcnt, toff, tstack, tgcount, theavy;
+    DBuf<double> theavy_part;
+    DBuf<unsigned char> tgflag;
+    DBuf<int2> tglist;
+    DBuf<unsigned char> tscan;
+    DBuf<double> tres, twsum;
     DBuf<float> probe_sink;
 
     PinnedBuf h_in, h_out, h_err;
@@ -503,12 +517,124 @@ static SortedF32 sorted32(sphgrav_ctx *c)
 }
 
 // The per-call pipeline on device-resident inputs and outputs.
+// Barnes-Hut mode: the preparation of the direct path (validation, Morton
+// sort, gather), then the octree, its multipoles, the group walk and the
+// scatter of the requested rows.  One particle set per call.
+static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
+                    int ni, const InputsDev &in, const OutputsDev &out, double *W, int nkernel)
+{
+    if (offsets.size() != 2)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "the tree mode takes one particle set per call");
+    if (c->capturing)
+        return set_err(SPHGRAV_ERR_PROTOCOL,
+                       "the tree mode cannot be captured: its build synchronises once per level");
+    TRY(prepare(c, offsets, full_rows, i_lo, ni, SPHGRAV_FP64, 0));
+    const Plan &P = c->plan;
+    cudaStream_t st = c->stream;
+    const int n = P.ntot;
+    if (n == 0) return SPHGRAV_OK;
+    SortedF64 D = sorted64(c);
+    SortedF32 F = sorted32(c);
+    CUDA_TRY(launch_validate(in, n, c->err.p, st));
+    CUDA_TRY(launch_bbox(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, st));
+    CUDA_TRY(launch_morton(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, P.bits, c->keys_in.p,
+                           c->vals_in.p, st));
+    CUDA_TRY(launch_sort(c->sort_temp.p, c->sort_temp.cap, c->keys_in.p, c->keys_out.p,
+                         c->vals_in.p, c->vals_out.p, n, P.end_bit, st));
+    CUDA_TRY(launch_gather(c->sets.p, P.nsets, P.max_npad, in, c->vals_out.p, D, F, st));
+    TRY(ensure(c, c->tcnt, (size_t)n + 1, "tree scratch"));
+    TRY(ensure(c, c->toff, (size_t)n + 1, "tree scratch"));
+    TRY(ensure(c, c->tscan, tree_scan_temp_bytes(n + 1), "tree scan"));
+    TRY(ensure(c, c->tnodes, std::max<size_t>(c->tnodes.cap, 2 * (size_t)n + 64), "tree nodes"));
+    int nn = 0, depth = 0;
+    for (;;) {
+        TRY(ensure(c, c->tgflag, c->tnodes.cap, "tree groups"));
+        TreeBuildArgs t;
+        t.n = n;
+        t.keys = c->keys_out.p;
+        t.nodes = c->tnodes.p;
+        t.cap = (int)std::min<size_t>(c->tnodes.cap, 0x7fffffff);
+        t.cnt = c->tcnt.p;
+        t.off = c->toff.p;
+        t.scan_temp = c->tscan.p;
+        t.scan_temp_bytes = c->tscan.cap;
+        t.gflag = c->tgflag.p;
+        const cudaError_t e = tree_build(t, &nn, &depth, st);
+        if (e == cudaErrorMemoryAllocation) {
+            TRY(ensure(c, c->tnodes, 2 * c->tnodes.cap, "tree nodes"));
+            continue;
+        }
+        CUDA_TRY(e);
+        break;
+    }
+    // walking groups: maximal nodes with <= TREE_GROUP particles
+    TRY(ensure(c, c->tglist, (size_t)n, "tree groups"));
+    TRY(ensure(c, c->tgcount, 2, "tree groups"));  // [0] groups, [1] heavy groups
+    CUDA_TRY(tree_groups(nn, c->tnodes.p, c->tgflag.p, c->tglist.p, c->tgcount.p, st));
+    int ngroups = 0;
+    CUDA_TRY(cudaMemcpyAsync(&ngroups, c->tgcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    TRY(ensure(c, c->tgeom, (size_t)nn, "tree geometry"));
+    TRY(ensure(c, c->tmp, (size_t)nn, "tree multipoles"));
+    CUDA_TRY(tree_props(nn, c->tnodes.p, D, c->theta, c->tgeom.p, c->tmp.p, st));
+    TRY(ensure(c, c->tstack, (size_t)tree_walk_warps(c->sm_count) * TREE_STACK, "tree stack"));
+    TRY(ensure(c, c->tres, 4 * (size_t)n, "tree results"));
+    CUDA_TRY(cudaMemsetAsync(c->head.p, 0, sizeof(int), st));
+    TreeWalkArgs a;
+    a.nodes = c->tnodes.p;
+    a.geom = c->tgeom.p;
+    a.mp = c->tmp.p;
+    a.D = D;
+    a.n = n;
+    a.ngroups = ngroups;
+    a.groups = c->tglist.p;
+    TRY(ensure(c, c->theavy, (size_t)std::max(ngroups, 1), "tree heavy groups"));
+    CUDA_TRY(cudaMemsetAsync(c->tgcount.p + 1, 0, sizeof(int), st));
+    a.heavy = c->theavy.p;
+    a.nheavy = c->tgcount.p + 1;
+    a.nkernel = nkernel;
+    a.head = c->head.p;
+    a.stack = c->tstack.p;
+    a.stack_cap = TREE_STACK;
+    a.out = c->tres.p;
+    a.err = c->err.p;
+    const bool timed = c->profiling;
+    if (timed) {
+        if (c->prof_used == c->prof_events.size()) {
+            cudaEvent_t e0, e1;
+            CUDA_TRY(cudaEventCreate(&e0));
+            CUDA_TRY(cudaEventCreate(&e1));
+            c->prof_events.push_back({e0, e1});
+        }
+        CUDA_TRY(cudaEventRecord(c->prof_events[c->prof_used].first, st));
+    }
+    CUDA_TRY(tree_walk(a, c->sm_count, st));
+    // groups whose particles' softening spheres hold too many particles: direct FP64
+    int nheavy = 0;
+    CUDA_TRY(cudaMemcpyAsync(&nheavy, c->tgcount.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (nheavy > 0) {
+        TRY(ensure(c, c->theavy_part, (size_t)nheavy * tree_heavy_chunks(nheavy) * 4 * 32,
+                   "tree heavy sums"));
+        CUDA_TRY(tree_heavy(nheavy, c->theavy.p, c->tglist.p, D, n, nkernel, c->theavy_part.p,
+                            c->tres.p, st));
+    }
+    c->tree_groups_last = ngroups;
+    c->tree_heavy_last = nheavy;
+    if (timed) CUDA_TRY(cudaEventRecord(c->prof_events[c->prof_used++].second, st));
+    CUDA_TRY(tree_scatter(n, full_rows ? 0 : i_lo, full_rows ? n : ni, c->tres.p, D.orig, out, st));
+    if (W) CUDA_TRY(tree_wsum(n, c->tres.p, D.m, W, st));
+    return SPHGRAV_OK;
+}
+
 static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
                       int ni, const InputsDev &in, const OutputsDev &out, double *W, int nkernel,
                       int precision)
 {
     if (nkernel < 0 || nkernel > 2)
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "nkernel must be 0, 1 or 2 (got %d)", nkernel);
+    if (precision == SPHGRAV_TREE)
+        return run_tree(c, offsets, full_rows, i_lo, ni, in, out, W, nkernel);
     if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT)
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
     const int variant = choose_variant(c, precision, offsets, full_rows, ni);
@@ -579,6 +705,8 @@ static int read_device_error(sphgrav_ctx *c)
         return set_err(SPHGRAV_ERR_INVALID_INPUT,
                        "invalid particle data (mass <= 0, range2 == 0 or a non-finite value)");
     if (e & DEVERR_TIMEOUT) return set_err(SPHGRAV_ERR_DEVICE_TIMEOUT, "device wait timed out");
+    if (e & DEVERR_TREE)
+        return set_err(SPHGRAV_ERR_TOO_LARGE, "tree walk: traversal stack full (theta too small for N?)");
     return SPHGRAV_OK;
 }
 
@@ -795,6 +923,10 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->imeta.release(); c->jmeta.release(); c->items.release(); c->partials.release();
     c->wtile.release(); c->wdev.release(); c->kick_counter.release(); c->probe_sink.release();
     c->range2.release();
+    c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release();
+    c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();
+    c->twsum.release(); c->tgcount.release(); c->tgflag.release(); c->tglist.release();
+    c->theavy.release(); c->theavy_part.release();
     c->h_in.release(); c->h_out.release(); c->h_err.release();
     for (auto &e : c->prof_events) {
         cudaEventDestroy(e.first);
@@ -949,6 +1081,8 @@ int sphgrav_lasthalf(sphgrav_ctx *c, double *ax, double *ay, double *az, double 
     const int e = *(int *)c->h_err.p;
     if (e & DEVERR_INPUT) return set_err(SPHGRAV_ERR_INVALID_INPUT, "invalid particle data");
     if (e & DEVERR_TIMEOUT) return set_err(SPHGRAV_ERR_DEVICE_TIMEOUT, "device wait timed out");
+    if (e & DEVERR_TREE)
+        return set_err(SPHGRAV_ERR_TOO_LARGE, "tree walk: traversal stack full (theta too small for N?)");
     const int ni = c->pend_ni, i0 = c->pend_i0;
     if (ni > 0 && (!ax || !ay || !az || !pot))
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL output pointer");
@@ -1280,6 +1414,7 @@ int sphgrav_fp64_peak_probe(sphgrav_ctx *c, int iters, double *tflops)
 static sphgrav_ctx *g_legacy = nullptr;
 static int g_legacy_device = -1;
 static int g_legacy_precision = -1;
+static double g_legacy_theta = 0.3;
 
 static void legacy_fail(const char *where, int st)
 {
@@ -1293,7 +1428,8 @@ static int legacy_precision()
     if (g_legacy_precision < 0) {
         const char *e = getenv("SPHGRAV_PRECISION");
         g_legacy_precision = (e && (!strcmp(e, "fp64") || !strcmp(e, "FP64"))) ? SPHGRAV_FP64
-                                                                                : SPHGRAV_F32SPLIT;
+                             : (e && (!strcmp(e, "tree") || !strcmp(e, "TREE"))) ? SPHGRAV_TREE
+                                                                                 : SPHGRAV_F32SPLIT;
     }
     return g_legacy_precision;
 }
@@ -1305,13 +1441,32 @@ static sphgrav_ctx *legacy_ctx()
         if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) dev = 0;
         int st = sphgrav_create(&g_legacy, dev);
         if (st != SPHGRAV_OK) legacy_fail("context creation", st);
+        st = sphgrav_set_theta(g_legacy, g_legacy_theta);
+        if (st != SPHGRAV_OK) legacy_fail("gpu_init_dev_ theta", st);
     }
     return g_legacy;
 }
 
+int sphgrav_set_theta(sphgrav_ctx *c, double theta)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (!(theta >= 0.0 && theta <= 2.0))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "theta must be in [0, 2] (got %g)", theta);
+    c->theta = theta;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_tree_stats(sphgrav_ctx *c, int *groups, int *heavy)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (groups) *groups = c->tree_groups_last;
+    if (heavy) *heavy = c->tree_heavy_last;
+    return SPHGRAV_OK;
+}
+
 int sphgrav_legacy_set_precision(int precision)
 {
-    if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT)
+    if (precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT && precision != SPHGRAV_TREE)
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
     g_legacy_precision = precision;
     return SPHGRAV_OK;
@@ -1319,7 +1474,6 @@ int sphgrav_legacy_set_precision(int precision)
 
 void gpu_init_dev_(int *myrank, double *theta)
 {
-    (void)theta;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
         legacy_fail("gpu_init_dev_", set_err(SPHGRAV_ERR_NO_DEVICE, "no CUDA device"));
@@ -1333,6 +1487,9 @@ void gpu_init_dev_(int *myrank, double *theta)
     g_legacy_device = dev;
     if (cudaSetDevice(dev) != cudaSuccess)
         legacy_fail("gpu_init_dev_", set_err(SPHGRAV_ERR_CUDA, "cudaSetDevice(%d) failed", dev));
+    // the opening angle of the tree mode (the direct modes do not use it)
+    if (theta) g_legacy_theta = *theta;
+    if (g_legacy) sphgrav_set_theta(g_legacy, g_legacy_theta);
 }
 
 void firsthalf_grav_forces_(int *n, int *n_lower, int *my_length, double *px, double *py,

@@ -65,6 +65,7 @@ struct ITileMeta {
 enum : int {
     DEVERR_INPUT = 1,
     DEVERR_TIMEOUT = 2,
+    DEVERR_TREE = 4,  // tree walk: traversal stack full
 };
 
 // Self-potential constants c of the zero-distance rule (cpu_grav.f:141,

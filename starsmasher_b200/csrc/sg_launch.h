@@ -92,4 +92,80 @@ cudaError_t launch_fp32_probe(int iters, int blocks, float *sink, cudaStream_t s
 cudaError_t launch_fp64_probe(int iters, int blocks, float *sink, cudaStream_t st);
 cudaError_t launch_wait_selftest(uint32_t polls, int *err, cudaStream_t st);
 
+// --- Barnes-Hut octree (sg_tree.cu)
+constexpr int TREE_LEAF = 16;    // a node with more particles splits
+constexpr int TREE_LEVELS = 21;  // Morton bits per axis
+constexpr int TREE_STACK = 8192; // traversal stack entries per warp
+constexpr int TREE_GROUP = 32;   // a walking group: a maximal node with <= 32 particles
+constexpr int TREE_BUDGET = 32768;  // particle-list entries a group may take before it is
+                                    // handed to the direct FP64 sum (a dense region inside
+                                    // one particle's softening length, e.g. a core point mass)
+constexpr int TREE_HEAVY_CHUNKS = 128;  // most source chunks of a heavy group's direct sum
+// Source chunks per heavy group: about 2048 blocks in all, 1..TREE_HEAVY_CHUNKS each.
+inline int tree_heavy_chunks(int nheavy)
+{
+    const int c = (2048 + nheavy - 1) / (nheavy > 0 ? nheavy : 1);
+    return c < 1 ? 1 : (c > TREE_HEAVY_CHUNKS ? TREE_HEAVY_CHUNKS : c);
+}
+
+struct TreeNode {
+    int start, end;     // sorted-slot range of its particles
+    int child, nchild;  // first child (children are contiguous), count; 0: leaf
+};
+struct NodeGeom {      // bounding box and opening data (48 bytes)
+    double cx, cy, cz; // box centre
+    float hx, hy, hz;  // half sizes, rounded up
+    float op2;         // (l / theta)^2, l = edge length
+    float h2max;       // largest H^2 of its particles
+    float pad_;
+};
+struct NodeMP {        // multipoles (64 bytes)
+    double mx, my, mz; // centre of mass
+    double m;          // mass
+    float s[6];        // second moment about the centre of mass: xx yy zz xy xz yz
+    float pad_[2];
+};
+struct TreeBuildArgs {
+    int n;
+    const unsigned long long *keys;  // sorted Morton keys of the n particles
+    TreeNode *nodes;
+    int cap;                         // node capacity
+    int *cnt, *off;                  // per-level scratch (n + 1 entries)
+    unsigned char *gflag;            // per node: a walking group (maximal with <= TREE_GROUP)
+    void *scan_temp;
+    size_t scan_temp_bytes;
+};
+struct TreeWalkArgs {
+    const TreeNode *nodes;
+    const NodeGeom *geom;
+    const NodeMP *mp;
+    SortedF64 D;
+    int n, ngroups, nkernel;
+    const int2 *groups;  // [ngroups] sorted-slot ranges (start, end), end - start <= 32
+    int *head;       // group counter (zeroed before the launch)
+    int *heavy;      // [ngroups] groups handed to the direct sum ...
+    int *nheavy;     // ... and their count (zeroed before the launch)
+    int *stack;      // TREE_STACK entries per walking warp
+    int stack_cap;
+    double *out;     // [4][n] in sorted order
+    int *err;
+};
+size_t tree_scan_temp_bytes(int n);
+// Builds the octree; returns cudaErrorMemoryAllocation (nothing else
+// changed) when `cap` nodes do not suffice.  Synchronises once per level.
+cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, cudaStream_t st);
+// Lists the walking groups (order not significant); *ngroups via `count`.
+cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag, int2 *glist,
+                        int *count, cudaStream_t st);
+cudaError_t tree_props(int nn, const TreeNode *nodes, const SortedF64 &D, double theta,
+                       NodeGeom *geom, NodeMP *mp, cudaStream_t st);
+int tree_walk_warps(int sm_count);
+cudaError_t tree_walk(const TreeWalkArgs &a, int sm_count, cudaStream_t st);
+cudaError_t tree_scatter(int n, int i_lo, int ni, const double *res, const int *orig,
+                         const OutputsDev &out, cudaStream_t st);
+cudaError_t tree_wsum(int n, const double *res, const double *m, double *W, cudaStream_t st);
+// Direct FP64 sums (all n sources) for the groups the walk handed over.
+cudaError_t tree_heavy(int nheavy, const int *heavy, const int2 *groups, const SortedF64 &D, int n,
+                       int nkernel, double *partials, double *out, cudaStream_t st);
+
 }  // namespace sg

@@ -1,0 +1,674 @@
+// sg_tree.cu -- Barnes-Hut octree gravity for sm_100a: the approximate
+// alternative that the reference ships as a drop-in library with the same
+// C-ABI (misc/SPHgravtree_lib: grav_force_tree.cu over libSequoia), written
+// here from its semantics:
+//   * an octree over the Morton-sorted particles; a node splits while it
+//     holds more than TREE_LEAF particles (the reference: 64);
+//   * every node carries its mass, centre of mass and second moment about
+//     it (monopole + quadrupole, as libSequoia's body_node);
+//   * particles are walked in groups, one warp each: the largest nodes that
+//     hold at most 32 particles (a leaf that cannot split is cut into chunks
+//     of 32); a node is opened when the gap between the group's and the
+//     node's bounding boxes is at most l / theta, l the node's edge length
+//     (libSequoia's minimum-distance criterion, compute_properties.cu:339,
+//     dev_shared_traverse_functions.cu:311-337); theta comes from
+//     gpu_init_dev_ (main.f:269-270 passes 0.3).  It is also opened when the
+//     gap is at most max(H) of the node's or the group's particles, so every
+//     pair closer than the softening length is evaluated particle by
+//     particle with the softened kernel (the reference leaves that test out,
+//     INDSOFT); with theta -> 0 the walk is therefore the direct sum;
+//   * accepted nodes interact through the quadrupole expansion, opened
+//     leaves particle by particle: FP32 for Newtonian pairs, FP64 with the
+//     CPU-path formulas (pair_f64_core) for r < max(H_i, H_j) and r = 0;
+//   * a group whose particle list passes TREE_BUDGET entries (its particles'
+//     softening spheres hold that many particles, e.g. a point-mass core with
+//     a large H) leaves the walk and gets the direct FP64 sum over all
+//     particles instead, spread over many CTAs (k_tree_heavy).
+// Construction is level by level with prefix sums (no atomics), and every
+// reduction has a fixed order: results are bit-for-bit reproducible.
+#include "sg_launch.h"
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+
+namespace sg {
+
+// ---------------------------------------------------------------- build
+__device__ __forceinline__ int lower_bound_key(const unsigned long long *keys, int lo, int hi,
+                                               unsigned long long v)
+{
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Children of node i of level `level` (keys of its particles share their
+// top 3*level Morton bits): the eight 3-bit digits of level + 1 split its
+// sorted range; b[0..8] are the digit boundaries.
+__device__ __forceinline__ void child_bounds(const TreeNode &T, int level,
+                                             const unsigned long long *keys, int b[9])
+{
+    const int sh = 3 * (TREE_LEVELS - 1 - level);  // digit of level + 1
+    const unsigned long long base = (keys[T.start] >> (sh + 3)) << (sh + 3);
+    b[0] = T.start;
+    b[8] = T.end;
+    for (int d = 1; d < 8; d++)
+        b[d] = lower_bound_key(keys, b[d - 1], T.end, base | ((unsigned long long)d << sh));
+}
+
+__global__ void k_tree_count(int l0, int l1, int level, const TreeNode *nodes,
+                             const unsigned long long *keys, int *cnt)
+{
+    const int i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= l1) return;
+    const TreeNode T = nodes[i];
+    int c = 0;
+    if (T.end - T.start > TREE_LEAF && level < TREE_LEVELS) {
+        int b[9];
+        child_bounds(T, level, keys, b);
+        for (int d = 0; d < 8; d++) c += b[d + 1] > b[d] ? 1 : 0;
+    }
+    cnt[i - l0] = c;
+}
+
+__global__ void k_tree_emit(int l0, int l1, int level, TreeNode *nodes,
+                            const unsigned long long *keys, const int *cnt, const int *off,
+                            int next_base, unsigned char *gflag)
+{
+    const int i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= l1) return;
+    const int c = cnt[i - l0];
+    TreeNode T = nodes[i];
+    if (c == 0) return;
+    int b[9];
+    child_bounds(T, level, keys, b);
+    int k = next_base + off[i - l0];
+    T.child = k;
+    T.nchild = c;
+    nodes[i] = T;
+    const bool big = T.end - T.start > TREE_GROUP;
+    for (int d = 0; d < 8; d++) {
+        if (b[d + 1] > b[d]) {
+            TreeNode C;
+            C.start = b[d];
+            C.end = b[d + 1];
+            C.child = 0;
+            C.nchild = 0;
+            gflag[k] = big && C.end - C.start <= TREE_GROUP;
+            nodes[k++] = C;
+        }
+    }
+}
+
+// Walking groups: every maximal node with at most TREE_GROUP particles, and
+// TREE_GROUP-particle chunks of the (coincident-particle) leaves that hold
+// more; each particle lies in exactly one.  Atomic order: results do not
+// depend on which warp walks which group.
+__global__ void k_tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag,
+                              int2 *glist, int *count)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        const TreeNode T = nodes[i];
+        if (gflag[i]) {
+            glist[atomicAdd(count, 1)] = make_int2(T.start, T.end);
+        } else if (T.nchild == 0 && T.end - T.start > TREE_GROUP) {
+            for (int b = T.start; b < T.end; b += TREE_GROUP)
+                glist[atomicAdd(count, 1)] = make_int2(b, min(b + TREE_GROUP, T.end));
+        }
+    }
+}
+
+__global__ void k_tree_root(TreeNode *nodes, int n, unsigned char *gflag)
+{
+    gflag[0] = n <= TREE_GROUP;
+    TreeNode R;
+    R.start = 0;
+    R.end = n;
+    R.child = 0;
+    R.nchild = 0;
+    nodes[0] = R;
+}
+
+// ------------------------------------------------------------ properties
+// One block of PROPS_WARPS warps per node: mass, centre of mass, bounds and
+// the largest H^2 of its particles in FP64, then the second moment about the
+// centre of mass; fixed-order reductions (warp shuffles, then the warps in
+// order), so the moments are reproducible.
+constexpr int PROPS_WARPS = 4;
+
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], const bool (&ismax)[NV],
+                                             double (*sh)[PROPS_WARPS])
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1)
+        for (int q = 0; q < NV; q++) {
+            const double u = __shfl_xor_sync(0xffffffffu, v[q], o);
+            v[q] = ismax[q] ? fmax(v[q], u) : v[q] + u;
+        }
+    if (lane == 0)
+        for (int q = 0; q < NV; q++) sh[q][w] = v[q];
+    __syncthreads();
+    for (int q = 0; q < NV; q++) {
+        double r = sh[q][0];
+        for (int k = 1; k < PROPS_WARPS; k++) r = ismax[q] ? fmax(r, sh[q][k]) : r + sh[q][k];
+        v[q] = r;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(PROPS_WARPS * 32)
+k_tree_props(int nn, const TreeNode *nodes, SortedF64 D, double theta, NodeGeom *geom, NodeMP *mp)
+{
+    __shared__ double sh[11][PROPS_WARPS];
+    const int i = blockIdx.x;
+    if (i >= nn) return;
+    const TreeNode T = nodes[i];
+    // m, mx, my, mz, h2max, -xlo, -ylo, -zlo, xhi, yhi, zhi (minima as negated maxima)
+    double v[11] = {0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY, -INFINITY, -INFINITY, -INFINITY, -INFINITY,
+                    -INFINITY};
+    const bool mx11[11] = {false, false, false, false, true, true, true, true, true, true, true};
+    for (int s = T.start + (int)threadIdx.x; s < T.end; s += PROPS_WARPS * 32) {
+        const double w = D.m[s], x = D.x[s], y = D.y[s], z = D.z[s];
+        v[0] += w;
+        v[1] += w * x;
+        v[2] += w * y;
+        v[3] += w * z;
+        v[4] = fmax(v[4], D.h2[s]);
+        v[5] = fmax(v[5], -x); v[6] = fmax(v[6], -y); v[7] = fmax(v[7], -z);
+        v[8] = fmax(v[8], x);  v[9] = fmax(v[9], y);  v[10] = fmax(v[10], z);
+    }
+    block_reduce<11>(v, mx11, sh);
+    const double m = v[0], cx = v[1] / m, cy = v[2] / m, cz = v[3] / m;
+    double q6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
+    const bool mx6[6] = {false, false, false, false, false, false};
+    for (int j = T.start + (int)threadIdx.x; j < T.end; j += PROPS_WARPS * 32) {
+        const double w = D.m[j], x = D.x[j] - cx, y = D.y[j] - cy, z = D.z[j] - cz;
+        q6[0] += w * x * x;
+        q6[1] += w * y * y;
+        q6[2] += w * z * z;
+        q6[3] += w * x * y;
+        q6[4] += w * x * z;
+        q6[5] += w * y * z;
+    }
+    block_reduce<6>(q6, mx6, sh);
+    if (threadIdx.x == 0) {
+        const double lo[3] = {-v[5], -v[6], -v[7]}, hi[3] = {v[8], v[9], v[10]};
+        NodeGeom G;
+        G.cx = 0.5 * (lo[0] + hi[0]);
+        G.cy = 0.5 * (lo[1] + hi[1]);
+        G.cz = 0.5 * (lo[2] + hi[2]);
+        // half sizes rounded up by 2^-20 of the coordinates' magnitude, so
+        // that float rounding never lets a node look farther than it is
+        const double c3[3] = {G.cx, G.cy, G.cz};
+        float hs[3];
+        double hmax = 0.0;
+        for (int d = 0; d < 3; d++) {
+            const double h = 0.5 * (hi[d] - lo[d]);
+            hs[d] = (float)(h + 9.5367e-7 * (fabs(c3[d]) + h));
+            hmax = fmax(hmax, h);
+        }
+        G.hx = hs[0];
+        G.hy = hs[1];
+        G.hz = hs[2];
+        const double l = 2.0 * hmax;  // edge length
+        G.op2 = l > 0.0 ? (theta > 0.0 ? (float)((l / theta) * (l / theta)) : INFINITY) : 0.f;
+        G.h2max = (float)v[4] * 1.000001f;
+        G.pad_ = 0.f;
+        geom[i] = G;
+        NodeMP P;
+        P.mx = cx;
+        P.my = cy;
+        P.mz = cz;
+        P.m = m;
+        for (int q = 0; q < 6; q++) P.s[q] = (float)q6[q];
+        P.pad_[0] = P.pad_[1] = 0.f;
+        mp[i] = P;
+    }
+}
+
+// -------------------------------------------------------------------- walk
+constexpr int WALK_WARPS = 4;
+constexpr int CELL_CAP = 64;  // < 32 pending + 32 appended per step
+constexpr int PART_CAP = 64;
+
+__global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
+{
+    __shared__ float s_cell[WALK_WARPS][10][CELL_CAP];  // x y z m sxx syy szz sxy sxz syz
+    __shared__ float s_part[WALK_WARPS][5][PART_CAP];   // x y z m H^2
+    __shared__ int s_pslot[WALK_WARPS][PART_CAP];
+    __shared__ int s_q[WALK_WARPS][64];               // FP64 pairs: owner lane << 8 | entry
+    __shared__ double s_qres[WALK_WARPS][4][32];      // their results
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    int *stack = a.stack + (size_t)(blockIdx.x * WALK_WARPS + w) * a.stack_cap;
+    const SortedF64 D = a.D;
+    float(*cl)[CELL_CAP] = s_cell[w];
+    float(*pl)[PART_CAP] = s_part[w];
+    int *ps = s_pslot[w];
+    int *q = s_q[w];
+    double(*qr)[32] = s_qres[w];
+
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = atomicAdd(a.head, 1);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= a.ngroups) break;
+        const int2 grp = a.groups[g];
+        const int s0 = grp.x;
+        const int s = s0 + lane;
+        const bool act = s < grp.y;
+        const int sr = act ? s : s0;  // inactive lanes mirror the group's first particle
+        const double px = D.x[sr], py = D.y[sr], pz = D.z[sr];
+        double lo[3] = {px, py, pz}, hi[3] = {px, py, pz};
+        float gh2 = act ? (float)D.h2[s] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) {
+            for (int d = 0; d < 3; d++) {
+                lo[d] = fmin(lo[d], __shfl_xor_sync(FULL, lo[d], o));
+                hi[d] = fmax(hi[d], __shfl_xor_sync(FULL, hi[d], o));
+            }
+            gh2 = fmaxf(gh2, __shfl_xor_sync(FULL, gh2, o));
+        }
+        gh2 *= 1.000001f;
+        const double cx = 0.5 * (lo[0] + hi[0]), cy = 0.5 * (lo[1] + hi[1]),
+                     cz = 0.5 * (lo[2] + hi[2]);
+        const float ghx = (float)(0.5 * (hi[0] - lo[0]) * (1.0 + 1e-6) + 1e-30);
+        const float ghy = (float)(0.5 * (hi[1] - lo[1]) * (1.0 + 1e-6) + 1e-30);
+        const float ghz = (float)(0.5 * (hi[2] - lo[2]) * (1.0 + 1e-6) + 1e-30);
+        const float xi = (float)(px - cx), yi = (float)(py - cy), zi = (float)(pz - cz);
+        const float h2i = act ? (float)D.h2[s] : 0.f;
+        // sums: each list flush in FP32, flushes and FP64 near pairs in FP64
+        double fx = 0.0, fy = 0.0, fz = 0.0, fp = 0.0;
+        int ncell = 0, npart = 0, top = 1;
+        int taken = 0;  // particle-list entries of this group so far
+        bool overflow = false, heavy = false;
+        if (lane == 0) stack[0] = 0;
+        __syncwarp();
+
+        auto eval_cells = [&]() {
+            if (act) {
+                float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
+                for (int e = 0; e < ncell; e++) {
+                    const float dx = cl[0][e] - xi, dy = cl[1][e] - yi, dz = cl[2][e] - zi;
+                    const float M = cl[3][e];
+                    const float sxx = cl[4][e], syy = cl[5][e], szz = cl[6][e];
+                    const float sxy = cl[7][e], sxz = cl[8][e], syz = cl[9][e];
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    const float ri = rsqrtf(r2);
+                    const float ri2 = ri * ri, ri3 = ri2 * ri, ri5 = ri3 * ri2;
+                    const float sdx = sxx * dx + sxy * dy + sxz * dz;
+                    const float sdy = sxy * dx + syy * dy + syz * dz;
+                    const float sdz = sxz * dx + syz * dy + szz * dz;
+                    const float dsd = dx * sdx + dy * sdy + dz * sdz;
+                    const float tr = sxx + syy + szz;
+                    // a = M d/r^3 - 3 S d/r^5 + 7.5 (d.S.d) d/r^7 - 1.5 tr(S) d/r^5
+                    const float cd = M * ri3 + (7.5f * dsd * ri2 - 1.5f * tr) * ri5;
+                    ax += cd * dx - 3.f * ri5 * sdx;
+                    ay += cd * dy - 3.f * ri5 * sdy;
+                    az += cd * dz - 3.f * ri5 * sdz;
+                    // phi = -M/r - 1.5 (d.S.d)/r^5 + 0.5 tr(S)/r^3
+                    pot += -M * ri - 1.5f * dsd * ri5 + 0.5f * tr * ri3;
+                }
+                fx += ax;
+                fy += ay;
+                fz += az;
+                fp += pot;
+            }
+            ncell = 0;
+            __syncwarp();
+        };
+        // FP64 pairs queued as (owner lane, list entry), evaluated one per lane
+        // and summed by each owner in queue order
+        auto eval_queue = [&](int cnt) {
+            if (lane < cnt) {
+                const int o = q[lane] >> 8, e = q[lane] & 255;
+                const int si = s0 + o, j = ps[e];
+                const PairOut r = pair_f64_core(D, a.nkernel, si, j, D.x[j] - D.x[si],
+                                                D.y[j] - D.y[si], D.z[j] - D.z[si], D.m[j],
+                                                D.h2[si], D.h2[j]);
+                qr[0][lane] = r.ax;
+                qr[1][lane] = r.ay;
+                qr[2][lane] = r.az;
+                qr[3][lane] = r.pot;
+            }
+            __syncwarp();
+            for (int t = 0; t < cnt; t++) {
+                if ((q[t] >> 8) == lane) {
+                    fx += qr[0][t];
+                    fy += qr[1][t];
+                    fz += qr[2][t];
+                    fp += qr[3][t];
+                }
+            }
+            __syncwarp();
+        };
+        auto eval_parts = [&]() {
+            float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
+            int nq = 0;
+            for (int e = 0; e < npart; e++) {
+                const float dx = pl[0][e] - xi, dy = pl[1][e] - yi, dz = pl[2][e] - zi;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool near = act && !(r2 >= fmaxf(h2i, pl[4][e]));
+                if (act && !near) {
+                    const float ri = rsqrtf(r2);
+                    const float mr = pl[3][e] * ri;
+                    const float mr3 = mr * ri * ri;
+                    ax += mr3 * dx;
+                    ay += mr3 * dy;
+                    az += mr3 * dz;
+                    pot -= mr;
+                }
+                const unsigned nm = __ballot_sync(FULL, near);
+                if (near) q[nq + __popc(nm & below)] = (lane << 8) | e;
+                nq += __popc(nm);
+                __syncwarp();
+                if (nq >= 32) {
+                    eval_queue(32);
+                    const int rest = nq - 32;  // < 32: move them to the front
+                    const int v = lane < rest ? q[32 + lane] : 0;
+                    __syncwarp();
+                    if (lane < rest) q[lane] = v;
+                    nq = rest;
+                    __syncwarp();
+                }
+            }
+            if (nq > 0) eval_queue(nq);
+            fx += ax;
+            fy += ay;
+            fz += az;
+            fp += pot;
+            npart = 0;
+            __syncwarp();
+        };
+
+        while (top > 0 && !heavy) {
+            const int nb = min(top, 32);
+            top -= nb;
+            const int node = lane < nb ? stack[top + lane] : -1;
+            __syncwarp();  // popped before the pushes below overwrite the slots
+            bool cell = false, leaf_open = false;
+            int nch = 0, ch0 = 0;
+            if (node >= 0) {
+                const NodeGeom G = a.geom[node];
+                const float gx = fmaxf(0.f, (float)fabs(G.cx - cx) - (G.hx + ghx));
+                const float gy = fmaxf(0.f, (float)fabs(G.cy - cy) - (G.hy + ghy));
+                const float gz = fmaxf(0.f, (float)fabs(G.cz - cz) - (G.hz + ghz));
+                const float d2 = gx * gx + gy * gy + gz * gz;
+                const bool open = d2 <= G.op2 || d2 <= fmaxf(G.h2max, gh2);
+                const TreeNode T = a.nodes[node];
+                cell = !open;
+                if (open) {
+                    if (T.nchild > 0) {
+                        nch = T.nchild;
+                        ch0 = T.child;
+                    } else {
+                        leaf_open = true;
+                    }
+                }
+            }
+            // accepted nodes join the cell list (group-relative coordinates)
+            const unsigned cm = __ballot_sync(FULL, cell);
+            if (cell) {
+                const int p = ncell + __popc(cm & below);
+                const NodeMP P = a.mp[node];
+                cl[0][p] = (float)(P.mx - cx);
+                cl[1][p] = (float)(P.my - cy);
+                cl[2][p] = (float)(P.mz - cz);
+                cl[3][p] = (float)P.m;
+                for (int q = 0; q < 6; q++) cl[4 + q][p] = P.s[q];
+            }
+            ncell += __popc(cm);
+            __syncwarp();
+            if (ncell >= 32) eval_cells();
+            // opened inner nodes push their children
+            int incl = nch;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int pushed = __shfl_sync(FULL, incl, 31);
+            if (top + pushed > a.stack_cap) {
+                overflow = true;
+                break;
+            }
+            for (int c = 0; c < nch; c++) stack[top + incl - nch + c] = ch0 + c;
+            top += pushed;
+            __syncwarp();
+            // opened leaves: their particles join the particle list
+            unsigned lm = __ballot_sync(FULL, leaf_open);
+            while (lm) {
+                const int src = __ffs(lm) - 1;
+                lm &= lm - 1;
+                const int ln = __shfl_sync(FULL, node, src);
+                const TreeNode T = a.nodes[ln];
+                taken += T.end - T.start;
+                if (taken > TREE_BUDGET) {
+                    heavy = true;  // hand the group to the direct sum
+                    break;
+                }
+                for (int b = T.start; b < T.end; b += 32) {
+                    const int j = b + lane;
+                    const bool has = j < T.end;
+                    if (has) {
+                        const int p = npart + lane;
+                        pl[0][p] = (float)(D.x[j] - cx);
+                        pl[1][p] = (float)(D.y[j] - cy);
+                        pl[2][p] = (float)(D.z[j] - cz);
+                        pl[3][p] = (float)D.m[j];
+                        pl[4][p] = (float)D.h2[j] * 1.000001f;
+                        ps[p] = j;
+                    }
+                    npart += __popc(__ballot_sync(FULL, has));
+                    __syncwarp();
+                    if (npart >= 32) eval_parts();
+                }
+            }
+        }
+        if (heavy) {
+            if (lane == 0) a.heavy[atomicAdd(a.nheavy, 1)] = g;
+            __syncwarp();
+            continue;
+        }
+        if (ncell > 0) eval_cells();
+        if (npart > 0) eval_parts();
+        if (overflow && lane == 0) atomicOr(a.err, DEVERR_TREE);
+        if (act) {
+            a.out[s] = fx;
+            a.out[a.n + s] = fy;
+            a.out[2 * a.n + s] = fz;
+            a.out[3 * a.n + s] = fp;
+        }
+    }
+}
+
+// Direct FP64 sum of a heavy group: block (h, c) sums the group's <= 32
+// particles (lane = row) over source chunk c (the block's warps take
+// interleaved sources); warps combine in order, chunks merge in order.
+constexpr int HEAVY_WARPS = 8;
+__global__ void __launch_bounds__(HEAVY_WARPS * 32)
+k_tree_heavy(const int *heavy, const int2 *groups, SortedF64 D, int n, int nkernel, int nchunks,
+             double *partials)
+{
+    __shared__ double sh[HEAVY_WARPS][4][32];
+    const int h = blockIdx.x, c = blockIdx.y;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int2 grp = groups[heavy[h]];
+    const int si = grp.x + lane;
+    const bool act = si < grp.y;
+    const int jb = (int)((long long)n * c / nchunks);
+    const int je = (int)((long long)n * (c + 1) / nchunks);
+    double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+    if (act) {
+        const double xi = D.x[si], yi = D.y[si], zi = D.z[si], h2i = D.h2[si];
+        for (int j = jb + w; j < je; j += HEAVY_WARPS) {
+            const PairOut o = pair_f64_core(D, nkernel, si, j, D.x[j] - xi, D.y[j] - yi,
+                                            D.z[j] - zi, D.m[j], h2i, D.h2[j]);
+            sx += o.ax;
+            sy += o.ay;
+            sz += o.az;
+            sp += o.pot;
+        }
+    }
+    sh[w][0][lane] = sx;
+    sh[w][1][lane] = sy;
+    sh[w][2][lane] = sz;
+    sh[w][3][lane] = sp;
+    __syncthreads();
+    if (w == 0) {
+        for (int q = 0; q < 4; q++) {
+            double v = sh[0][q][lane];
+            for (int k = 1; k < HEAVY_WARPS; k++) v += sh[k][q][lane];
+            partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane] = v;
+        }
+    }
+}
+
+__global__ void k_tree_heavy_merge(int nheavy, const int *heavy, const int2 *groups, int nchunks,
+                                   const double *partials, int n, double *out)
+{
+    const int h = blockIdx.x, lane = threadIdx.x;
+    if (h >= nheavy) return;
+    const int2 grp = groups[heavy[h]];
+    const int si = grp.x + lane;
+    if (si >= grp.y) return;
+    for (int q = 0; q < 4; q++) {
+        double v = 0.0;
+        for (int c = 0; c < nchunks; c++)
+            v += partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane];
+        out[(size_t)q * n + si] = v;
+    }
+}
+
+cudaError_t tree_heavy(int nheavy, const int *heavy, const int2 *groups, const SortedF64 &D, int n,
+                       int nkernel, double *partials, double *out, cudaStream_t st)
+{
+    if (nheavy <= 0) return cudaSuccess;
+    const int nchunks = tree_heavy_chunks(nheavy);
+    k_tree_heavy<<<dim3(nheavy, nchunks), HEAVY_WARPS * 32, 0, st>>>(heavy, groups, D, n, nkernel,
+                                                                    nchunks, partials);
+    ++g_launches;
+    k_tree_heavy_merge<<<nheavy, 32, 0, st>>>(nheavy, heavy, groups, nchunks, partials, n, out);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+// Sorted-order results to the caller's rows [i_lo, i_lo + ni).
+__global__ void k_tree_scatter(int n, int i_lo, int ni, const double *res, const int *orig,
+                               OutputsDev out)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int p = orig[s];
+        if (p < i_lo || p >= i_lo + ni) continue;
+        out.ax[p] = res[s];
+        out.ay[p] = res[n + s];
+        out.az[p] = res[2 * n + s];
+        out.pot[p] = res[3 * n + s];
+    }
+}
+
+// W = 1/2 sum m phi over the particles, one block, fixed order.
+__global__ void k_tree_wsum(int n, const double *res, const double *m, double *W)
+{
+    __shared__ double part[1024];
+    double w = 0.0;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) w += m[s] * res[3 * n + s];
+    part[threadIdx.x] = w;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *W = 0.5 * part[0];
+}
+
+cudaError_t tree_wsum(int n, const double *res, const double *m, double *W, cudaStream_t st)
+{
+    k_tree_wsum<<<1, 1024, 0, st>>>(n, res, m, W);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- driver
+size_t tree_scan_temp_bytes(int n)
+{
+    size_t b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (const int *)nullptr, (int *)nullptr, std::max(n, 1));
+    return b;
+}
+
+cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, cudaStream_t st)
+{
+    cudaError_t e;
+    k_tree_root<<<1, 1, 0, st>>>(t.nodes, t.n, t.gflag);
+    ++g_launches;
+    int l0 = 0, l1 = 1, level = 0;
+    while (l1 > l0) {
+        const int cnt_n = l1 - l0;
+        const int blocks = (cnt_n + 255) / 256;
+        k_tree_count<<<blocks, 256, 0, st>>>(l0, l1, level, t.nodes, t.keys, t.cnt);
+        ++g_launches;
+        size_t tb = t.scan_temp_bytes;
+        if ((e = cub::DeviceScan::ExclusiveSum(t.scan_temp, tb, t.cnt, t.off, cnt_n, st)) != cudaSuccess)
+            return e;
+        // children of this level = off[last] + cnt[last]
+        int tail[2];
+        if ((e = cudaMemcpyAsync(&tail[0], t.off + cnt_n - 1, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return e;
+        if ((e = cudaMemcpyAsync(&tail[1], t.cnt + cnt_n - 1, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+        const int nchild = tail[0] + tail[1];
+        if (nchild == 0) break;
+        if ((long long)l1 + nchild > t.cap) return cudaErrorMemoryAllocation;  // caller grows and retries
+        k_tree_emit<<<blocks, 256, 0, st>>>(l0, l1, level, t.nodes, t.keys, t.cnt, t.off, l1, t.gflag);
+        ++g_launches;
+        l0 = l1;
+        l1 += nchild;
+        ++level;
+    }
+    *nnodes = l1;
+    *depth = level;
+    return cudaGetLastError();
+}
+
+cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag, int2 *glist,
+                        int *count, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    k_tree_groups<<<std::min((nn + 255) / 256, 4096), 256, 0, st>>>(nn, nodes, gflag, glist, count);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t tree_props(int nn, const TreeNode *nodes, const SortedF64 &D, double theta,
+                       NodeGeom *geom, NodeMP *mp, cudaStream_t st)
+{
+    k_tree_props<<<nn, PROPS_WARPS * 32, 0, st>>>(nn, nodes, D, theta, geom, mp);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+int tree_walk_warps(int sm_count) { return sm_count * 8 * WALK_WARPS; }
+
+cudaError_t tree_walk(const TreeWalkArgs &a, int sm_count, cudaStream_t st)
+{
+    k_tree_walk<<<sm_count * 8, WALK_WARPS * 32, 0, st>>>(a);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t tree_scatter(int n, int i_lo, int ni, const double *res, const int *orig,
+                         const OutputsDev &out, cudaStream_t st)
+{
+    k_tree_scatter<<<std::min((n + 255) / 256, 4096), 256, 0, st>>>(n, i_lo, ni, res, orig, out);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+}  // namespace sg

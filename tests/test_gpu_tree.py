@@ -1,0 +1,213 @@
+"""Barnes-Hut tree mode (SPHGRAV_TREE) against the direct sum.
+
+The reference ships its tree code as a second library behind the same C-ABI
+(misc/SPHgravtree_lib: grav_force_tree.cu), with the opening angle passed by
+gpu_init_dev_ (main.f:269-270).  Its answers are approximations whose error
+is set by theta, so the tests here bound that error against this library's
+FP64 direct sum (itself <= 1e-12 of the oracle) instead of asking for
+equality:
+  theta = 0        opens every node: the direct sum, acc and pot <= 2e-6
+  theta = 0.3/0.5/0.7  acc RMS <= 1e-4 / 5e-4 / 1e-3, max <= 3e-3 / 1.5e-2 / 3e-2
+and check what must hold exactly: bit-for-bit reproducible results, row
+slices equal to the full call's rows, groups handed to the direct FP64 sum
+(a point-mass core whose softening sphere holds most of the star) exact to
+1e-10, and the calls that tree mode refuses.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import err_report
+from starsmasher_b200 import _lib, api, inputs
+
+pytestmark = pytest.mark.gpu
+
+BOUNDS = {0.3: (1e-4, 3e-3, 1e-5), 0.5: (5e-4, 1.5e-2, 5e-5), 0.7: (1e-3, 3e-2, 1e-4)}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def dev(a):
+    return _torch().as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+@pytest.fixture(scope="module")
+def star16k():
+    return inputs.cached("config1")
+
+
+@pytest.fixture(scope="module")
+def direct16k(star16k):
+    from starsmasher_b200 import Context
+    s = star16k
+    with Context(0) as c:
+        return {k: c.forces(s.x, s.y, s.z, s.m, s.range2, k, "fp64") for k in (0, 1, 2)}
+
+
+def _tree(ctx, s, theta, nkernel=0, **kw):
+    ctx.set_theta(theta)
+    try:
+        return ctx.forces(s.x, s.y, s.z, s.m, s.range2, nkernel, "tree", **kw)
+    finally:
+        ctx.set_theta(0.3)
+
+
+@pytest.mark.parametrize("nkernel", [0, 1, 2])
+def test_theta_zero_is_the_direct_sum(gpu_ctx, star16k, direct16k, nkernel):
+    got = _tree(gpu_ctx, star16k, 0.0, nkernel)
+    r = err_report(*got, *direct16k[nkernel])
+    assert r["acc_max"] <= 2e-6 and r["pot_max"] <= 2e-6, r
+    assert r["acc_max_ill"] <= 1e-4, r
+
+
+def test_error_bounded_and_growing_with_theta(gpu_ctx, star16k, direct16k):
+    rms = []
+    for theta, (b_rms, b_max, b_pot) in BOUNDS.items():
+        r = err_report(*_tree(gpu_ctx, star16k, theta), *direct16k[0])
+        assert r["acc_rms"] <= b_rms and r["acc_max"] <= b_max and r["pot_rms"] <= b_pot, (theta, r)
+        rms.append(r["acc_rms"])
+    assert rms == sorted(rms)
+
+
+def test_deterministic_and_row_slice(gpu_ctx, star16k):
+    s = star16k
+    a = _tree(gpu_ctx, s, 0.5)
+    b = _tree(gpu_ctx, s, 0.5)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+    lo, ni = 3001, 5003
+    gpu_ctx.set_theta(0.5)
+    try:
+        gpu_ctx.firsthalf(s.x, s.y, s.z, s.m, s.range2, 0, "tree", lo, ni)
+        outs = gpu_ctx.lasthalf(*(np.full(s.n, 7.0) for _ in range(4)))
+    finally:
+        gpu_ctx.set_theta(0.3)
+    for u, v in zip(outs, a):
+        assert np.array_equal(u[lo:lo + ni], v[lo:lo + ni])
+        assert np.all(u[:lo] == 7.0) and np.all(u[lo + ni:] == 7.0)
+
+
+def test_heavy_group_is_exact(gpu_ctx):
+    """A point-mass core with 2 hp = 0.1 in an n=3 polytrope: about 2/3 of
+    the particles lie inside its softening sphere, so its walking group is
+    handed to the direct FP64 sum and its row is exact."""
+    s = inputs.red_giant(65536, seed=5)
+    want = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "fp64")
+    got = _tree(gpu_ctx, s, 0.5)
+    groups, heavy = gpu_ctx.tree_stats()
+    assert heavy >= 1 and groups > 1000
+    core = 0  # the core is particle 0
+    for u, v in zip(got, want):
+        assert abs(u[core] - v[core]) <= 1e-10 * abs(v[core])
+    r = err_report(*got, *want)
+    assert r["acc_rms"] <= 1e-3 and r["acc_max"] <= 5e-2, r
+    again = _tree(gpu_ctx, s, 0.5)
+    for u, v in zip(got, again):
+        assert np.array_equal(u, v)
+
+
+def test_energy_per_set(gpu_ctx, star16k):
+    t = _torch()
+    s = star16k
+    X = [dev(a) for a in (s.x, s.y, s.z, s.m, s.range2)]
+    outs = [t.zeros(s.n, dtype=t.float64, device="cuda") for _ in range(4)]
+    W = t.zeros(1, dtype=t.float64, device="cuda")
+    gpu_ctx.set_theta(0.5)
+    try:
+        gpu_ctx.forces_device(s.n, *X, *outs, W=W, precision="tree")
+        gpu_ctx.sync()
+    finally:
+        gpu_ctx.set_theta(0.3)
+    pot = outs[3].cpu().numpy()
+    assert W.item() == pytest.approx(0.5 * np.sum(s.m * pot), rel=1e-12)
+
+
+@pytest.mark.parametrize("nkernel", [0, 1, 2])
+def test_edge_cases(gpu_ctx, nkernel):
+    """Coincident particles, point masses, one particle, a set whose keys all
+    coincide (a leaf that cannot split), ragged sizes; theta = 0 vs the oracle.
+    Newtonian pairs are FP32 and these small random sets have partly
+    cancelling sums: 5e-6 of |a| (2.2e-6 seen at n = 33)."""
+    rng = np.random.default_rng(17 + nkernel)
+    cases = [(np.array([0.0, 0.0, 0.3, 0.3, 1.0]), np.array([0.0, 0.0, 0.1, 0.1, -0.2]), np.zeros(5),
+              np.array([1.0, 2.0, 0.5, 0.5, 0.1]), np.array([0.25, 0.0625, 0.04, -0.04, 0.5])),
+             (np.zeros(1), np.zeros(1), np.zeros(1), np.ones(1), np.ones(1))]
+    same = np.full(100, 0.25)
+    cases.append((same, same.copy(), same.copy(), rng.uniform(0.1, 1.0, 100), np.full(100, 0.01)))
+    for n in (31, 33, 1029, 4097):
+        p = rng.normal(size=(n, 3))
+        mm = rng.uniform(0.1, 1.0, n) / n
+        rr = rng.uniform(0.01, 2.0, n) ** 2
+        rr[::13] *= -1
+        p[5] = p[9]
+        cases.append((p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), mm, rr))
+    gpu_ctx.set_theta(0.0)
+    try:
+        for (x, y, z, m, r2) in cases:
+            got = gpu_ctx.forces(x, y, z, m, r2, nkernel, "tree")
+            o = oracle.triangle(x, y, z, m, r2, nkernel)
+            amag = np.sqrt(o[0] ** 2 + o[1] ** 2 + o[2] ** 2)
+            da = np.sqrt((got[0] - o[0]) ** 2 + (got[1] - o[1]) ** 2 + (got[2] - o[2]) ** 2)
+            ok = da <= 5e-6 * amag + 1e-13 * np.max(amag)
+            assert ok.all(), (x.shape[0], np.max(da / np.maximum(amag, 1e-300)))
+            np.testing.assert_allclose(got[3], o[3], rtol=5e-6, atol=0)
+    finally:
+        gpu_ctx.set_theta(0.3)
+
+
+def test_empty_set(gpu_ctx):
+    e = np.zeros(0)
+    got = gpu_ctx.forces(e, e, e, e, e, 0, "tree")
+    assert all(a.shape == (0,) for a in got)
+
+
+def test_refusals(gpu_ctx, star16k):
+    s = star16k
+    for bad in (-0.1, 2.5, float("nan")):
+        with pytest.raises(_lib.SphgravError) as e:
+            gpu_ctx.set_theta(bad)
+        assert e.value.status == _lib.ERR_INVALID_ARGUMENT
+    b = inputs.batch_models(3, 500, 1500, seed=71)
+    with pytest.raises(_lib.SphgravError) as e:
+        gpu_ctx.batch_forces(b.offsets, b.x, b.y, b.z, b.m, b.range2, 0, "tree")
+    assert e.value.status == _lib.ERR_INVALID_ARGUMENT
+    t = _torch()
+    X = [dev(a) for a in (s.x, s.y, s.z, s.m, s.range2)]
+    outs = [t.zeros(s.n, dtype=t.float64, device="cuda") for _ in range(4)]
+    gpu_ctx.forces_device(s.n, *X, *outs, precision="tree")
+    gpu_ctx.sync()
+    with pytest.raises(_lib.SphgravError) as e:
+        with gpu_ctx.capture():
+            gpu_ctx.forces_device(s.n, *X, *outs, precision="tree")
+    assert e.value.status == _lib.ERR_PROTOCOL
+    gpu_ctx.sync()
+    # the context stays usable
+    got = _tree(gpu_ctx, s, 0.5)
+    assert np.all(np.isfinite(got[0]))
+
+
+def test_legacy_abi_takes_theta_from_gpu_init_dev(gpu_ctx, star16k):
+    """gpu_init_dev_(myrank, theta) sets the opening angle of the legacy
+    calls (main.f:269-270); the results equal the context API's at that theta."""
+    s = star16k
+    n = s.n
+    try:
+        api.set_legacy_precision("tree")
+        prev = None
+        for theta in (0.5, 0.7):
+            api.gpu_init_dev(0, theta)
+            api.firsthalf_grav_forces(n, 1, n, s.x, s.y, s.z, s.m, s.range2, q=1, nkernel=0)
+            outs = [np.zeros(n) for _ in range(4)]
+            api.lasthalf_grav_forces(n, *outs)
+            want = _tree(gpu_ctx, s, theta)
+            for u, v in zip(outs, want):
+                assert np.array_equal(u, v)
+            if prev is not None:
+                assert not np.array_equal(prev, outs[0])
+            prev = outs[0]
+    finally:
+        api.gpu_init_dev(0, 0.3)
+        api.set_legacy_precision("f32split")
