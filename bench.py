@@ -62,6 +62,9 @@ def parse():
                         "(seeded 1e-3 position kick + gravity) on device-resident state")
     p.add_argument("--no-separate", action="store_true",
                    help="batched workloads: skip the one-call-per-set comparison")
+    p.add_argument("--tree-thetas", default="0.3,0.5",
+                   help="single-set workloads: opening angles of the Barnes-Hut tree "
+                        "section ('' skips it); accuracy against the FP64 kernel")
     return p.parse_args()
 
 
@@ -416,6 +419,7 @@ def main():
     # --------------------------------------------- FP64 kernel and accuracy
     fp64 = None
     acc = None
+    res64 = None
     if not args.no_fp64:
         step("fp64")
         torch.cuda.synchronize()
@@ -438,6 +442,36 @@ def main():
                              "frac": ach64 / peak64, "flops_per_pair": FLOPS_PER_PAIR,
                              "time": "whole step (preparation included)",
                              "peak_source": "measured in-run: DFMA throughput probe on this GPU"}}
+
+    # ------------------------------------- Barnes-Hut tree (approximate)
+    tree = None
+    thetas = [float(v) for v in args.tree_thetas.split(",") if v.strip()]
+    if not batched and thetas and res64 is not None:
+        tree = {"what": "SPHGRAV_TREE: octree, quadrupole nodes, FP64 softened pairs; "
+                        "approximate, error set by theta (not the direct-sum metric)",
+                "time": "whole call, device arrays (build syncs once per tree level)",
+                "direct_f32split_ms_per_step": ms_per_step}
+        for th in thetas:
+            ctx.set_theta(th)
+            gravity("tree")
+            torch.cuda.synchronize()
+            res_t = [o.cpu().numpy() for o in outs]
+            ngroups, nheavy = ctx.tree_stats()
+            reps = 3
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                gravity("tree")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms_t = e0.elapsed_time(e1) / reps
+            tree[f"theta_{th:g}"] = {
+                "ms_per_step": ms_t, "speedup_vs_f32split_direct": ms_per_step / ms_t,
+                "speedup_vs_fp64_direct": fp64["ms_per_step"] / ms_t,
+                "walking_groups": ngroups, "groups_direct_fp64": nheavy,
+                "accuracy_vs_fp64": accuracy(res_t, res64)}
+        ctx.set_theta(0.3)
 
     # ------------------------------------------------------------ roofline
     peak = ctx.fp32_peak_probe(200000)
@@ -521,6 +555,8 @@ def main():
             line["batch_vs_separate"] = batch_cmp
         if graph_info:
             line["graph_sweep"] = graph_info
+        if tree:
+            line["tree"] = tree
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -223,9 +223,9 @@ int sphgrav_set_fp64_band(sphgrav_ctx *ctx, double factor);
  * node and gives the direct sum. */
 int sphgrav_set_theta(sphgrav_ctx *ctx, double theta);
 /* SPHGRAV_TREE: walking groups of the last tree call and how many of them
- * were handed to the direct FP64 sum (groups whose particles' softening
- * spheres hold more than 32,768 particles; their rows are exact direct
- * sums).  Either pointer may be NULL. */
+ * were handed to the direct FP64 sum (groups with more than 8,192 particles
+ * within the largest H of their box; their rows are exact direct sums).
+ * Either pointer may be NULL. */
 int sphgrav_tree_stats(sphgrav_ctx *ctx, int *groups, int *heavy);
 /* Force a kernel variant by index (-1 = automatic) for a precision. */
 int sphgrav_force_variant(sphgrav_ctx *ctx, int precision, int variant);

@@ -187,7 +187,7 @@ struct sphgrav_ctx {
     DBuf<NodeGeom> tgeom;
     DBuf<NodeMP> tmp;
     DBuf<int> tcnt, toff, tstack, tgcount, theavy;
-    DBuf<double> theavy_part;
+    DBuf<double> theavy_part, tacc;
     DBuf<unsigned char> tgflag;
     DBuf<int2> tglist;
     DBuf<unsigned char> tscan;
@@ -547,6 +547,7 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     TRY(ensure(c, c->tscan, tree_scan_temp_bytes(n + 1), "tree scan"));
     TRY(ensure(c, c->tnodes, std::max<size_t>(c->tnodes.cap, 2 * (size_t)n + 64), "tree nodes"));
     int nn = 0, depth = 0;
+    int level_start[TREE_LEVELS + 2];
     for (;;) {
         TRY(ensure(c, c->tgflag, c->tnodes.cap, "tree groups"));
         TreeBuildArgs t;
@@ -559,7 +560,7 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
         t.scan_temp = c->tscan.p;
         t.scan_temp_bytes = c->tscan.cap;
         t.gflag = c->tgflag.p;
-        const cudaError_t e = tree_build(t, &nn, &depth, st);
+        const cudaError_t e = tree_build(t, &nn, &depth, level_start, st);
         if (e == cudaErrorMemoryAllocation) {
             TRY(ensure(c, c->tnodes, 2 * c->tnodes.cap, "tree nodes"));
             continue;
@@ -576,7 +577,9 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     CUDA_TRY(cudaStreamSynchronize(st));
     TRY(ensure(c, c->tgeom, (size_t)nn, "tree geometry"));
     TRY(ensure(c, c->tmp, (size_t)nn, "tree multipoles"));
-    CUDA_TRY(tree_props(nn, c->tnodes.p, D, c->theta, c->tgeom.p, c->tmp.p, st));
+    TRY(ensure(c, c->tacc, tree_acc_bytes(nn) / sizeof(double), "tree node sums"));
+    CUDA_TRY(tree_props(nn, c->tnodes.p, D, c->theta, level_start, depth, c->tacc.p, c->tgeom.p,
+                        c->tmp.p, st));
     TRY(ensure(c, c->tstack, (size_t)tree_walk_warps(c->sm_count) * TREE_STACK, "tree stack"));
     TRY(ensure(c, c->tres, 4 * (size_t)n, "tree results"));
     CUDA_TRY(cudaMemsetAsync(c->head.p, 0, sizeof(int), st));
@@ -614,7 +617,7 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     CUDA_TRY(cudaMemcpyAsync(&nheavy, c->tgcount.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     if (nheavy > 0) {
-        TRY(ensure(c, c->theavy_part, (size_t)nheavy * tree_heavy_chunks(nheavy) * 4 * 32,
+        TRY(ensure(c, c->theavy_part, (size_t)nheavy * tree_heavy_chunks(nheavy, n) * 4 * 32,
                    "tree heavy sums"));
         CUDA_TRY(tree_heavy(nheavy, c->theavy.p, c->tglist.p, D, n, nkernel, c->theavy_part.p,
                             c->tres.p, st));
@@ -926,7 +929,7 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release();
     c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();
     c->twsum.release(); c->tgcount.release(); c->tgflag.release(); c->tglist.release();
-    c->theavy.release(); c->theavy_part.release();
+    c->theavy.release(); c->theavy_part.release(); c->tacc.release();
     c->h_in.release(); c->h_out.release(); c->h_err.release();
     for (auto &e : c->prof_events) {
         cudaEventDestroy(e.first);

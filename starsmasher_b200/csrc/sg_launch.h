@@ -97,14 +97,16 @@ constexpr int TREE_LEAF = 16;    // a node with more particles splits
 constexpr int TREE_LEVELS = 21;  // Morton bits per axis
 constexpr int TREE_STACK = 8192; // traversal stack entries per warp
 constexpr int TREE_GROUP = 32;   // a walking group: a maximal node with <= 32 particles
-constexpr int TREE_BUDGET = 32768;  // particle-list entries a group may take before it is
-                                    // handed to the direct FP64 sum (a dense region inside
-                                    // one particle's softening length, e.g. a core point mass)
-constexpr int TREE_HEAVY_CHUNKS = 128;  // most source chunks of a heavy group's direct sum
-// Source chunks per heavy group: about 2048 blocks in all, 1..TREE_HEAVY_CHUNKS each.
-inline int tree_heavy_chunks(int nheavy)
+constexpr int TREE_BUDGET = 8192;  // particles within the largest H of a group's box (each
+                                   // tested pair by pair) before the group is handed to the
+                                   // direct FP64 sum; a typical group has ~500-800
+constexpr int TREE_HEAVY_CHUNKS = 1024;  // most source chunks of a heavy group's direct sum
+// Source chunks per heavy group: about 4096 blocks in all, at least 2048 sources
+// each, 1..TREE_HEAVY_CHUNKS.
+inline int tree_heavy_chunks(int nheavy, int n)
 {
-    const int c = (2048 + nheavy - 1) / (nheavy > 0 ? nheavy : 1);
+    int c = (4096 + nheavy - 1) / (nheavy > 0 ? nheavy : 1);
+    if (c > n / 2048) c = n / 2048;
     return c < 1 ? 1 : (c > TREE_HEAVY_CHUNKS ? TREE_HEAVY_CHUNKS : c);
 }
 
@@ -153,12 +155,18 @@ struct TreeWalkArgs {
 size_t tree_scan_temp_bytes(int n);
 // Builds the octree; returns cudaErrorMemoryAllocation (nothing else
 // changed) when `cap` nodes do not suffice.  Synchronises once per level.
-cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, cudaStream_t st);
+// level_start: TREE_LEVELS + 2 entries; nodes of level l are [level_start[l], level_start[l + 1]),
+// levels 0..depth.
+cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, int *level_start,
+                       cudaStream_t st);
 // Lists the walking groups (order not significant); *ngroups via `count`.
 cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag, int2 *glist,
                         int *count, cudaStream_t st);
+// Node properties; acc_buf: tree_acc_bytes(nn) of scratch.
+size_t tree_acc_bytes(int nn);
 cudaError_t tree_props(int nn, const TreeNode *nodes, const SortedF64 &D, double theta,
-                       NodeGeom *geom, NodeMP *mp, cudaStream_t st);
+                       const int *level_start, int depth, void *acc_buf, NodeGeom *geom,
+                       NodeMP *mp, cudaStream_t st);
 int tree_walk_warps(int sm_count);
 cudaError_t tree_walk(const TreeWalkArgs &a, int sm_count, cudaStream_t st);
 cudaError_t tree_scatter(int n, int i_lo, int ni, const double *res, const int *orig,

@@ -20,10 +20,10 @@
 //   * accepted nodes interact through the quadrupole expansion, opened
 //     leaves particle by particle: FP32 for Newtonian pairs, FP64 with the
 //     CPU-path formulas (pair_f64_core) for r < max(H_i, H_j) and r = 0;
-//   * a group whose particle list passes TREE_BUDGET entries (its particles'
-//     softening spheres hold that many particles, e.g. a point-mass core with
-//     a large H) leaves the walk and gets the direct FP64 sum over all
-//     particles instead, spread over many CTAs (k_tree_heavy).
+//   * a group with more than TREE_BUDGET particles within the largest H of
+//     its box (a dense region inside a softening sphere, e.g. a point-mass
+//     core with a large H) leaves the walk and gets the direct FP64 sum over
+//     all particles instead, spread over many CTAs (k_tree_heavy).
 // Construction is level by level with prefix sums (no atomics), and every
 // reduction has a fixed order: results are bit-for-bit reproducible.
 #include "sg_launch.h"
@@ -90,7 +90,11 @@ __global__ void k_tree_emit(int l0, int l1, int level, TreeNode *nodes,
     T.child = k;
     T.nchild = c;
     nodes[i] = T;
+    // Children of a node too big to be a group become groups, consecutive
+    // small siblings merged (Morton order) while they total <= TREE_GROUP:
+    // gflag of a run's first child = the run's length in nodes.
     const bool big = T.end - T.start > TREE_GROUP;
+    int run = -1, run_len = 0, run_n = 0;
     for (int d = 0; d < 8; d++) {
         if (b[d + 1] > b[d]) {
             TreeNode C;
@@ -98,23 +102,40 @@ __global__ void k_tree_emit(int l0, int l1, int level, TreeNode *nodes,
             C.end = b[d + 1];
             C.child = 0;
             C.nchild = 0;
-            gflag[k] = big && C.end - C.start <= TREE_GROUP;
+            const int cn = C.end - C.start;
+            gflag[k] = 0;
+            if (big && cn <= TREE_GROUP) {
+                if (run >= 0 && run_n + cn <= TREE_GROUP) {
+                    run_len++;
+                    run_n += cn;
+                } else {
+                    if (run >= 0) gflag[run] = (unsigned char)run_len;
+                    run = k;
+                    run_len = 1;
+                    run_n = cn;
+                }
+            } else if (run >= 0) {
+                gflag[run] = (unsigned char)run_len;
+                run = -1;
+            }
             nodes[k++] = C;
         }
     }
+    if (run >= 0) gflag[run] = (unsigned char)run_len;
 }
 
-// Walking groups: every maximal node with at most TREE_GROUP particles, and
-// TREE_GROUP-particle chunks of the (coincident-particle) leaves that hold
-// more; each particle lies in exactly one.  Atomic order: results do not
-// depend on which warp walks which group.
+// Walking groups: runs of consecutive sibling nodes that together hold at
+// most TREE_GROUP particles (each a maximal such node or merged with its
+// neighbours), and TREE_GROUP-particle chunks of the (coincident-particle)
+// leaves that hold more; each particle lies in exactly one.  Atomic order:
+// results do not depend on which warp walks which group.
 __global__ void k_tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag,
                               int2 *glist, int *count)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
         const TreeNode T = nodes[i];
         if (gflag[i]) {
-            glist[atomicAdd(count, 1)] = make_int2(T.start, T.end);
+            glist[atomicAdd(count, 1)] = make_int2(T.start, nodes[i + gflag[i] - 1].end);
         } else if (T.nchild == 0 && T.end - T.start > TREE_GROUP) {
             for (int b = T.start; b < T.end; b += TREE_GROUP)
                 glist[atomicAdd(count, 1)] = make_int2(b, min(b + TREE_GROUP, T.end));
@@ -134,101 +155,162 @@ __global__ void k_tree_root(TreeNode *nodes, int n, unsigned char *gflag)
 }
 
 // ------------------------------------------------------------ properties
-// One block of PROPS_WARPS warps per node: mass, centre of mass, bounds and
-// the largest H^2 of its particles in FP64, then the second moment about the
-// centre of mass; fixed-order reductions (warp shuffles, then the warps in
-// order), so the moments are reproducible.
-constexpr int PROPS_WARPS = 4;
+// Leaves from their particles (one warp each, fixed-order butterfly sums),
+// inner nodes from their children in child order, deepest level first
+// (masses and centres of mass combined, second moments moved to the new
+// centre by the parallel-axis rule), all in FP64: reproducible, and every
+// level costs one short launch instead of a pass over its particles.
+struct NodeAcc {
+    double m, c[3];   // mass, centre of mass
+    double lo[3], hi[3];
+    double s[6];      // second moment about c: xx yy zz xy xz yz
+    double h2max;
+};
 
-template <int NV>
-__device__ __forceinline__ void block_reduce(double (&v)[NV], const bool (&ismax)[NV],
-                                             double (*sh)[PROPS_WARPS])
+__device__ __forceinline__ double warp_sum(double v)
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1)
-        for (int q = 0; q < NV; q++) {
-            const double u = __shfl_xor_sync(0xffffffffu, v[q], o);
-            v[q] = ismax[q] ? fmax(v[q], u) : v[q] + u;
-        }
-    if (lane == 0)
-        for (int q = 0; q < NV; q++) sh[q][w] = v[q];
-    __syncthreads();
-    for (int q = 0; q < NV; q++) {
-        double r = sh[q][0];
-        for (int k = 1; k < PROPS_WARPS; k++) r = ismax[q] ? fmax(r, sh[q][k]) : r + sh[q][k];
-        v[q] = r;
-    }
-    __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
-__global__ void __launch_bounds__(PROPS_WARPS * 32)
-k_tree_props(int nn, const TreeNode *nodes, SortedF64 D, double theta, NodeGeom *geom, NodeMP *mp)
+__global__ void k_tree_leaf_acc(int nn, const TreeNode *nodes, SortedF64 D, NodeAcc *acc)
 {
-    __shared__ double sh[11][PROPS_WARPS];
-    const int i = blockIdx.x;
-    if (i >= nn) return;
-    const TreeNode T = nodes[i];
-    // m, mx, my, mz, h2max, -xlo, -ylo, -zlo, xhi, yhi, zhi (minima as negated maxima)
-    double v[11] = {0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY, -INFINITY, -INFINITY, -INFINITY, -INFINITY,
-                    -INFINITY};
-    const bool mx11[11] = {false, false, false, false, true, true, true, true, true, true, true};
-    for (int s = T.start + (int)threadIdx.x; s < T.end; s += PROPS_WARPS * 32) {
-        const double w = D.m[s], x = D.x[s], y = D.y[s], z = D.z[s];
-        v[0] += w;
-        v[1] += w * x;
-        v[2] += w * y;
-        v[3] += w * z;
-        v[4] = fmax(v[4], D.h2[s]);
-        v[5] = fmax(v[5], -x); v[6] = fmax(v[6], -y); v[7] = fmax(v[7], -z);
-        v[8] = fmax(v[8], x);  v[9] = fmax(v[9], y);  v[10] = fmax(v[10], z);
-    }
-    block_reduce<11>(v, mx11, sh);
-    const double m = v[0], cx = v[1] / m, cy = v[2] / m, cz = v[3] / m;
-    double q6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx yy zz xy xz yz
-    const bool mx6[6] = {false, false, false, false, false, false};
-    for (int j = T.start + (int)threadIdx.x; j < T.end; j += PROPS_WARPS * 32) {
-        const double w = D.m[j], x = D.x[j] - cx, y = D.y[j] - cy, z = D.z[j] - cz;
-        q6[0] += w * x * x;
-        q6[1] += w * y * y;
-        q6[2] += w * z * z;
-        q6[3] += w * x * y;
-        q6[4] += w * x * z;
-        q6[5] += w * y * z;
-    }
-    block_reduce<6>(q6, mx6, sh);
-    if (threadIdx.x == 0) {
-        const double lo[3] = {-v[5], -v[6], -v[7]}, hi[3] = {v[8], v[9], v[10]};
-        NodeGeom G;
-        G.cx = 0.5 * (lo[0] + hi[0]);
-        G.cy = 0.5 * (lo[1] + hi[1]);
-        G.cz = 0.5 * (lo[2] + hi[2]);
-        // half sizes rounded up by 2^-20 of the coordinates' magnitude, so
-        // that float rounding never lets a node look farther than it is
-        const double c3[3] = {G.cx, G.cy, G.cz};
-        float hs[3];
-        double hmax = 0.0;
-        for (int d = 0; d < 3; d++) {
-            const double h = 0.5 * (hi[d] - lo[d]);
-            hs[d] = (float)(h + 9.5367e-7 * (fabs(c3[d]) + h));
-            hmax = fmax(hmax, h);
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nn; i += nw) {
+        const TreeNode T = nodes[i];
+        if (T.nchild > 0) continue;
+        double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0, h2 = 0.0;
+        double nlo[3] = {-INFINITY, -INFINITY, -INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int s = T.start + lane; s < T.end; s += 32) {
+            const double w = D.m[s], x = D.x[s], y = D.y[s], z = D.z[s];
+            m += w;
+            mx += w * x;
+            my += w * y;
+            mz += w * z;
+            h2 = fmax(h2, D.h2[s]);
+            nlo[0] = fmax(nlo[0], -x); nlo[1] = fmax(nlo[1], -y); nlo[2] = fmax(nlo[2], -z);
+            hi[0] = fmax(hi[0], x);    hi[1] = fmax(hi[1], y);    hi[2] = fmax(hi[2], z);
         }
-        G.hx = hs[0];
-        G.hy = hs[1];
-        G.hz = hs[2];
-        const double l = 2.0 * hmax;  // edge length
-        G.op2 = l > 0.0 ? (theta > 0.0 ? (float)((l / theta) * (l / theta)) : INFINITY) : 0.f;
-        G.h2max = (float)v[4] * 1.000001f;
-        G.pad_ = 0.f;
-        geom[i] = G;
-        NodeMP P;
-        P.mx = cx;
-        P.my = cy;
-        P.mz = cz;
-        P.m = m;
-        for (int q = 0; q < 6; q++) P.s[q] = (float)q6[q];
-        P.pad_[0] = P.pad_[1] = 0.f;
-        mp[i] = P;
+        m = warp_sum(m);
+        mx = warp_sum(mx);
+        my = warp_sum(my);
+        mz = warp_sum(mz);
+        h2 = warp_max(h2);
+        for (int d = 0; d < 3; d++) {
+            nlo[d] = warp_max(nlo[d]);
+            hi[d] = warp_max(hi[d]);
+        }
+        // massless nodes sit at their box centre
+        const double cx = m > 0.0 ? mx / m : 0.5 * (hi[0] - nlo[0]);
+        const double cy = m > 0.0 ? my / m : 0.5 * (hi[1] - nlo[1]);
+        const double cz = m > 0.0 ? mz / m : 0.5 * (hi[2] - nlo[2]);
+        double q[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int s = T.start + lane; s < T.end; s += 32) {
+            const double w = D.m[s], x = D.x[s] - cx, y = D.y[s] - cy, z = D.z[s] - cz;
+            q[0] += w * x * x;
+            q[1] += w * y * y;
+            q[2] += w * z * z;
+            q[3] += w * x * y;
+            q[4] += w * x * z;
+            q[5] += w * y * z;
+        }
+        for (int k = 0; k < 6; k++) q[k] = warp_sum(q[k]);
+        if (lane == 0) {
+            NodeAcc A;
+            A.m = m;
+            A.c[0] = cx; A.c[1] = cy; A.c[2] = cz;
+            for (int d = 0; d < 3; d++) {
+                A.lo[d] = -nlo[d];
+                A.hi[d] = hi[d];
+            }
+            for (int k = 0; k < 6; k++) A.s[k] = q[k];
+            A.h2max = h2;
+            acc[i] = A;
+        }
     }
+}
+
+__global__ void k_tree_inner_acc(int l0, int l1, const TreeNode *nodes, NodeAcc *acc)
+{
+    const int i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= l1) return;
+    const TreeNode T = nodes[i];
+    if (T.nchild == 0) return;
+    NodeAcc A;
+    A.m = 0.0;
+    double mc[3] = {0.0, 0.0, 0.0};
+    A.h2max = 0.0;
+    for (int d = 0; d < 3; d++) {
+        A.lo[d] = INFINITY;
+        A.hi[d] = -INFINITY;
+    }
+    for (int k = 0; k < T.nchild; k++) {
+        const NodeAcc &C = acc[T.child + k];
+        A.m += C.m;
+        for (int d = 0; d < 3; d++) {
+            mc[d] += C.m * C.c[d];
+            A.lo[d] = fmin(A.lo[d], C.lo[d]);
+            A.hi[d] = fmax(A.hi[d], C.hi[d]);
+        }
+        A.h2max = fmax(A.h2max, C.h2max);
+    }
+    for (int d = 0; d < 3; d++) A.c[d] = A.m > 0.0 ? mc[d] / A.m : 0.5 * (A.lo[d] + A.hi[d]);
+    for (int q = 0; q < 6; q++) A.s[q] = 0.0;
+    for (int k = 0; k < T.nchild; k++) {
+        const NodeAcc &C = acc[T.child + k];
+        const double dx = C.c[0] - A.c[0], dy = C.c[1] - A.c[1], dz = C.c[2] - A.c[2];
+        A.s[0] += C.s[0] + C.m * dx * dx;
+        A.s[1] += C.s[1] + C.m * dy * dy;
+        A.s[2] += C.s[2] + C.m * dz * dz;
+        A.s[3] += C.s[3] + C.m * dx * dy;
+        A.s[4] += C.s[4] + C.m * dx * dz;
+        A.s[5] += C.s[5] + C.m * dy * dz;
+    }
+    acc[i] = A;
+}
+
+__global__ void k_tree_finalize(int nn, const NodeAcc *acc, double theta, NodeGeom *geom,
+                                NodeMP *mp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const NodeAcc A = acc[i];
+    NodeGeom G;
+    G.cx = 0.5 * (A.lo[0] + A.hi[0]);
+    G.cy = 0.5 * (A.lo[1] + A.hi[1]);
+    G.cz = 0.5 * (A.lo[2] + A.hi[2]);
+    // half sizes rounded up by 2^-20 of the coordinates' magnitude, so
+    // that float rounding never lets a node look farther than it is
+    const double c3[3] = {G.cx, G.cy, G.cz};
+    float hs[3];
+    double hmax = 0.0;
+    for (int d = 0; d < 3; d++) {
+        const double h = 0.5 * (A.hi[d] - A.lo[d]);
+        hs[d] = (float)(h + 9.5367e-7 * (fabs(c3[d]) + h));
+        hmax = fmax(hmax, h);
+    }
+    G.hx = hs[0];
+    G.hy = hs[1];
+    G.hz = hs[2];
+    const double l = 2.0 * hmax;  // edge length
+    G.op2 = l > 0.0 ? (theta > 0.0 ? (float)((l / theta) * (l / theta)) : INFINITY) : 0.f;
+    G.h2max = (float)A.h2max * 1.000001f;
+    G.pad_ = 0.f;
+    geom[i] = G;
+    NodeMP P;
+    P.mx = A.c[0];
+    P.my = A.c[1];
+    P.mz = A.c[2];
+    P.m = A.m;
+    for (int q = 0; q < 6; q++) P.s[q] = (float)A.s[q];
+    P.pad_[0] = P.pad_[1] = 0.f;
+    mp[i] = P;
 }
 
 // -------------------------------------------------------------------- walk
@@ -238,17 +320,22 @@ constexpr int PART_CAP = 64;
 
 __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
 {
-    __shared__ float s_cell[WALK_WARPS][10][CELL_CAP];  // x y z m sxx syy szz sxy sxz syz
-    __shared__ float s_part[WALK_WARPS][5][PART_CAP];   // x y z m H^2
+    // accepted nodes: {x y z M} {sxx syy szz sxy} {sxz syz - -}, group-relative
+    __shared__ float4 s_cell[WALK_WARPS][3][CELL_CAP];
+    // particles farther than any H from the whole group: {x y z m}
+    __shared__ float4 s_far[WALK_WARPS][PART_CAP];
+    // the other particles: x y z m H^2 and their sorted slot
+    __shared__ float s_part[WALK_WARPS][5][PART_CAP];
     __shared__ int s_pslot[WALK_WARPS][PART_CAP];
-    __shared__ int s_q[WALK_WARPS][64];               // FP64 pairs: owner lane << 8 | entry
-    __shared__ double s_qres[WALK_WARPS][4][32];      // their results
+    __shared__ int s_q[WALK_WARPS][64];           // FP64 pairs: owner lane << 8 | entry
+    __shared__ double s_qres[WALK_WARPS][4][32];  // their results
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
     int *stack = a.stack + (size_t)(blockIdx.x * WALK_WARPS + w) * a.stack_cap;
     const SortedF64 D = a.D;
-    float(*cl)[CELL_CAP] = s_cell[w];
+    float4(*cl)[CELL_CAP] = s_cell[w];
+    float4 *fl = s_far[w];
     float(*pl)[PART_CAP] = s_part[w];
     int *ps = s_pslot[w];
     int *q = s_q[w];
@@ -284,42 +371,65 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
         const float h2i = act ? (float)D.h2[s] : 0.f;
         // sums: each list flush in FP32, flushes and FP64 near pairs in FP64
         double fx = 0.0, fy = 0.0, fz = 0.0, fp = 0.0;
-        int ncell = 0, npart = 0, top = 1;
-        int taken = 0;  // particle-list entries of this group so far
+        int ncell = 0, nfar = 0, npart = 0, top = 1;
+        int taken = 0;  // tested-list entries of this group so far
         bool overflow = false, heavy = false;
         if (lane == 0) stack[0] = 0;
         __syncwarp();
 
+        // Every accepted node's box is disjoint from the group's (its gap is
+        // above zero), so r > 0 for every lane, the idle ones included (they
+        // mirror a particle of the group): no lane needs a guard.
         auto eval_cells = [&]() {
-            if (act) {
-                float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
-                for (int e = 0; e < ncell; e++) {
-                    const float dx = cl[0][e] - xi, dy = cl[1][e] - yi, dz = cl[2][e] - zi;
-                    const float M = cl[3][e];
-                    const float sxx = cl[4][e], syy = cl[5][e], szz = cl[6][e];
-                    const float sxy = cl[7][e], sxz = cl[8][e], syz = cl[9][e];
-                    const float r2 = dx * dx + dy * dy + dz * dz;
-                    const float ri = rsqrtf(r2);
-                    const float ri2 = ri * ri, ri3 = ri2 * ri, ri5 = ri3 * ri2;
-                    const float sdx = sxx * dx + sxy * dy + sxz * dz;
-                    const float sdy = sxy * dx + syy * dy + syz * dz;
-                    const float sdz = sxz * dx + syz * dy + szz * dz;
-                    const float dsd = dx * sdx + dy * sdy + dz * sdz;
-                    const float tr = sxx + syy + szz;
-                    // a = M d/r^3 - 3 S d/r^5 + 7.5 (d.S.d) d/r^7 - 1.5 tr(S) d/r^5
-                    const float cd = M * ri3 + (7.5f * dsd * ri2 - 1.5f * tr) * ri5;
-                    ax += cd * dx - 3.f * ri5 * sdx;
-                    ay += cd * dy - 3.f * ri5 * sdy;
-                    az += cd * dz - 3.f * ri5 * sdz;
-                    // phi = -M/r - 1.5 (d.S.d)/r^5 + 0.5 tr(S)/r^3
-                    pot += -M * ri - 1.5f * dsd * ri5 + 0.5f * tr * ri3;
-                }
-                fx += ax;
-                fy += ay;
-                fz += az;
-                fp += pot;
+            float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
+            for (int e = 0; e < ncell; e++) {
+                const float4 A = cl[0][e], B = cl[1][e], C = cl[2][e];
+                const float dx = A.x - xi, dy = A.y - yi, dz = A.z - zi;
+                const float M = A.w;
+                const float sxx = B.x, syy = B.y, szz = B.z, sxy = B.w, sxz = C.x, syz = C.y;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const float ri = rsqrtf(r2);
+                const float ri2 = ri * ri, ri3 = ri2 * ri, ri5 = ri3 * ri2;
+                const float sdx = sxx * dx + sxy * dy + sxz * dz;
+                const float sdy = sxy * dx + syy * dy + syz * dz;
+                const float sdz = sxz * dx + syz * dy + szz * dz;
+                const float dsd = dx * sdx + dy * sdy + dz * sdz;
+                const float tr = sxx + syy + szz;
+                // a = M d/r^3 - 3 S d/r^5 + 7.5 (d.S.d) d/r^7 - 1.5 tr(S) d/r^5
+                const float cd = M * ri3 + (7.5f * dsd * ri2 - 1.5f * tr) * ri5;
+                ax += cd * dx - 3.f * ri5 * sdx;
+                ay += cd * dy - 3.f * ri5 * sdy;
+                az += cd * dz - 3.f * ri5 * sdz;
+                // phi = -M/r - 1.5 (d.S.d)/r^5 + 0.5 tr(S)/r^3
+                pot += -M * ri - 1.5f * dsd * ri5 + 0.5f * tr * ri3;
             }
+            fx += ax;
+            fy += ay;
+            fz += az;
+            fp += pot;
             ncell = 0;
+            __syncwarp();
+        };
+        // Far particles: Newtonian FP32 pairs, no per-pair test (r > 0 as above).
+        auto eval_far = [&]() {
+            float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
+            for (int e = 0; e < nfar; e++) {
+                const float4 P = fl[e];
+                const float dx = P.x - xi, dy = P.y - yi, dz = P.z - zi;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const float ri = rsqrtf(r2);
+                const float mr = P.w * ri;
+                const float mr3 = mr * ri * ri;
+                ax += mr3 * dx;
+                ay += mr3 * dy;
+                az += mr3 * dz;
+                pot -= mr;
+            }
+            fx += ax;
+            fy += ay;
+            fz += az;
+            fp += pot;
+            nfar = 0;
             __syncwarp();
         };
         // FP64 pairs queued as (owner lane, list entry), evaluated one per lane
@@ -347,6 +457,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
             }
             __syncwarp();
         };
+        // Particles that may lie within some H of some lane: tested per pair,
+        // softened (or r = 0) pairs go to the FP64 queue.
         auto eval_parts = [&]() {
             float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
             int nq = 0;
@@ -416,11 +528,10 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
             if (cell) {
                 const int p = ncell + __popc(cm & below);
                 const NodeMP P = a.mp[node];
-                cl[0][p] = (float)(P.mx - cx);
-                cl[1][p] = (float)(P.my - cy);
-                cl[2][p] = (float)(P.mz - cz);
-                cl[3][p] = (float)P.m;
-                for (int q = 0; q < 6; q++) cl[4 + q][p] = P.s[q];
+                cl[0][p] = make_float4((float)(P.mx - cx), (float)(P.my - cy), (float)(P.mz - cz),
+                                       (float)P.m);
+                cl[1][p] = make_float4(P.s[0], P.s[1], P.s[2], P.s[3]);
+                cl[2][p] = make_float4(P.s[4], P.s[5], 0.f, 0.f);
             }
             ncell += __popc(cm);
             __syncwarp();
@@ -439,34 +550,55 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
             for (int c = 0; c < nch; c++) stack[top + incl - nch + c] = ch0 + c;
             top += pushed;
             __syncwarp();
-            // opened leaves: their particles join the particle list
+            // opened leaves: their particles join the far list or the tested list
             unsigned lm = __ballot_sync(FULL, leaf_open);
             while (lm) {
                 const int src = __ffs(lm) - 1;
                 lm &= lm - 1;
                 const int ln = __shfl_sync(FULL, node, src);
                 const TreeNode T = a.nodes[ln];
-                taken += T.end - T.start;
-                if (taken > TREE_BUDGET) {
-                    heavy = true;  // hand the group to the direct sum
-                    break;
-                }
                 for (int b = T.start; b < T.end; b += 32) {
                     const int j = b + lane;
                     const bool has = j < T.end;
+                    bool far = false;
+                    float ex = 0.f, ey = 0.f, ez = 0.f, em = 0.f, eh2 = 0.f;
                     if (has) {
-                        const int p = npart + lane;
-                        pl[0][p] = (float)(D.x[j] - cx);
-                        pl[1][p] = (float)(D.y[j] - cy);
-                        pl[2][p] = (float)(D.z[j] - cz);
-                        pl[3][p] = (float)D.m[j];
-                        pl[4][p] = (float)D.h2[j] * 1.000001f;
+                        ex = (float)(D.x[j] - cx);
+                        ey = (float)(D.y[j] - cy);
+                        ez = (float)(D.z[j] - cz);
+                        em = (float)D.m[j];
+                        eh2 = (float)D.h2[j] * 1.000001f;
+                        // a lower bound of the particle's distance to the group's
+                        // box (1e-6 covers the FP32 roundings of ex and this sum)
+                        const float bx = fmaxf(0.f, fabsf(ex) * (1.f - 1e-6f) - ghx);
+                        const float by = fmaxf(0.f, fabsf(ey) * (1.f - 1e-6f) - ghy);
+                        const float bz = fmaxf(0.f, fabsf(ez) * (1.f - 1e-6f) - ghz);
+                        far = (bx * bx + by * by + bz * bz) * 0.9999f > fmaxf(eh2, gh2);
+                    }
+                    const unsigned fm = __ballot_sync(FULL, has && far);
+                    const unsigned tm = __ballot_sync(FULL, has && !far);
+                    if (has && far) fl[nfar + __popc(fm & below)] = make_float4(ex, ey, ez, em);
+                    if (has && !far) {
+                        const int p = npart + __popc(tm & below);
+                        pl[0][p] = ex;
+                        pl[1][p] = ey;
+                        pl[2][p] = ez;
+                        pl[3][p] = em;
+                        pl[4][p] = eh2;
                         ps[p] = j;
                     }
-                    npart += __popc(__ballot_sync(FULL, has));
+                    nfar += __popc(fm);
+                    npart += __popc(tm);
+                    taken += __popc(tm);
                     __syncwarp();
+                    if (taken > TREE_BUDGET) {
+                        heavy = true;  // hand the group to the direct sum
+                        break;
+                    }
+                    if (nfar >= 32) eval_far();
                     if (npart >= 32) eval_parts();
                 }
+                if (heavy) break;
             }
         }
         if (heavy) {
@@ -475,6 +607,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
             continue;
         }
         if (ncell > 0) eval_cells();
+        if (nfar > 0) eval_far();
         if (npart > 0) eval_parts();
         if (overflow && lane == 0) atomicOr(a.err, DEVERR_TREE);
         if (act) {
@@ -528,31 +661,29 @@ k_tree_heavy(const int *heavy, const int2 *groups, SortedF64 D, int n, int nkern
     }
 }
 
+// warp q of block h: quantity q of heavy group h, chunks in order
 __global__ void k_tree_heavy_merge(int nheavy, const int *heavy, const int2 *groups, int nchunks,
                                    const double *partials, int n, double *out)
 {
-    const int h = blockIdx.x, lane = threadIdx.x;
+    const int h = blockIdx.x, lane = threadIdx.x & 31, q = threadIdx.x >> 5;
     if (h >= nheavy) return;
     const int2 grp = groups[heavy[h]];
     const int si = grp.x + lane;
     if (si >= grp.y) return;
-    for (int q = 0; q < 4; q++) {
-        double v = 0.0;
-        for (int c = 0; c < nchunks; c++)
-            v += partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane];
-        out[(size_t)q * n + si] = v;
-    }
+    double v = 0.0;
+    for (int c = 0; c < nchunks; c++) v += partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane];
+    out[(size_t)q * n + si] = v;
 }
 
 cudaError_t tree_heavy(int nheavy, const int *heavy, const int2 *groups, const SortedF64 &D, int n,
                        int nkernel, double *partials, double *out, cudaStream_t st)
 {
     if (nheavy <= 0) return cudaSuccess;
-    const int nchunks = tree_heavy_chunks(nheavy);
+    const int nchunks = tree_heavy_chunks(nheavy, n);
     k_tree_heavy<<<dim3(nheavy, nchunks), HEAVY_WARPS * 32, 0, st>>>(heavy, groups, D, n, nkernel,
                                                                     nchunks, partials);
     ++g_launches;
-    k_tree_heavy_merge<<<nheavy, 32, 0, st>>>(nheavy, heavy, groups, nchunks, partials, n, out);
+    k_tree_heavy_merge<<<nheavy, 128, 0, st>>>(nheavy, heavy, groups, nchunks, partials, n, out);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -601,13 +732,15 @@ size_t tree_scan_temp_bytes(int n)
     return b;
 }
 
-cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, cudaStream_t st)
+cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, int *level_start,
+                       cudaStream_t st)
 {
     cudaError_t e;
     k_tree_root<<<1, 1, 0, st>>>(t.nodes, t.n, t.gflag);
     ++g_launches;
     int l0 = 0, l1 = 1, level = 0;
     while (l1 > l0) {
+        level_start[level] = l0;
         const int cnt_n = l1 - l0;
         const int blocks = (cnt_n + 255) / 256;
         k_tree_count<<<blocks, 256, 0, st>>>(l0, l1, level, t.nodes, t.keys, t.cnt);
@@ -631,6 +764,7 @@ cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, cudaStre
         l1 += nchild;
         ++level;
     }
+    level_start[level + 1] = l1;
     *nnodes = l1;
     *depth = level;
     return cudaGetLastError();
@@ -646,10 +780,21 @@ cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gfla
     return cudaGetLastError();
 }
 
+size_t tree_acc_bytes(int nn) { return (size_t)nn * sizeof(NodeAcc); }
+
 cudaError_t tree_props(int nn, const TreeNode *nodes, const SortedF64 &D, double theta,
-                       NodeGeom *geom, NodeMP *mp, cudaStream_t st)
+                       const int *level_start, int depth, void *acc_buf, NodeGeom *geom,
+                       NodeMP *mp, cudaStream_t st)
 {
-    k_tree_props<<<nn, PROPS_WARPS * 32, 0, st>>>(nn, nodes, D, theta, geom, mp);
+    NodeAcc *acc = (NodeAcc *)acc_buf;
+    k_tree_leaf_acc<<<std::min((nn + 7) / 8, 148 * 16), 256, 0, st>>>(nn, nodes, D, acc);
+    ++g_launches;
+    for (int l = depth - 1; l >= 0; l--) {
+        const int l0 = level_start[l], l1 = level_start[l + 1];
+        k_tree_inner_acc<<<(l1 - l0 + 127) / 128, 128, 0, st>>>(l0, l1, nodes, acc);
+        ++g_launches;
+    }
+    k_tree_finalize<<<(nn + 255) / 256, 256, 0, st>>>(nn, acc, theta, geom, mp);
     ++g_launches;
     return cudaGetLastError();
 }
