@@ -124,7 +124,8 @@ struct NodeGeom {      // bounding box and opening data (48 bytes)
 struct NodeMP {        // multipoles (64 bytes)
     double mx, my, mz; // centre of mass
     double m;          // mass
-    float s[6];        // second moment about the centre of mass: xx yy zz xy xz yz
+    float q[6];        // traceless quadrupole 3 S - tr(S) I about the centre of
+                       // mass (S the second moment): xx yy zz xy xz yz
     float pad_[2];
 };
 struct TreeBuildArgs {

@@ -308,7 +308,12 @@ __global__ void k_tree_finalize(int nn, const NodeAcc *acc, double theta, NodeGe
     P.my = A.c[1];
     P.mz = A.c[2];
     P.m = A.m;
-    for (int q = 0; q < 6; q++) P.s[q] = (float)A.s[q];
+    // traceless quadrupole Q = 3 S - tr(S) I
+    const double tr = A.s[0] + A.s[1] + A.s[2];
+    P.q[0] = (float)(3.0 * A.s[0] - tr);
+    P.q[1] = (float)(3.0 * A.s[1] - tr);
+    P.q[2] = (float)(3.0 * A.s[2] - tr);
+    for (int q = 3; q < 6; q++) P.q[q] = (float)(3.0 * A.s[q]);
     P.pad_[0] = P.pad_[1] = 0.f;
     mp[i] = P;
 }
@@ -320,7 +325,7 @@ constexpr int PART_CAP = 64;
 
 __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
 {
-    // accepted nodes: {x y z M} {sxx syy szz sxy} {sxz syz - -}, group-relative
+    // accepted nodes, group-relative: {x y z M} {Qxx Qyy Qzz Qxy} {Qxz Qyz - -}
     __shared__ float4 s_cell[WALK_WARPS][3][CELL_CAP];
     // particles farther than any H from the whole group: {x y z m}
     __shared__ float4 s_far[WALK_WARPS][PART_CAP];
@@ -380,33 +385,34 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
         // Every accepted node's box is disjoint from the group's (its gap is
         // above zero), so r > 0 for every lane, the idle ones included (they
         // mirror a particle of the group): no lane needs a guard.
+        //   a = M d/r^3 - Q d/r^5 + 2.5 (d.Q.d) d/r^7,  phi = -M/r - 0.5 (d.Q.d)/r^5
         auto eval_cells = [&]() {
-            float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
+            float ax = 0.f, ay = 0.f, az = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, pm = 0.f, pq = 0.f;
             for (int e = 0; e < ncell; e++) {
                 const float4 A = cl[0][e], B = cl[1][e], C = cl[2][e];
                 const float dx = A.x - xi, dy = A.y - yi, dz = A.z - zi;
-                const float M = A.w;
-                const float sxx = B.x, syy = B.y, szz = B.z, sxy = B.w, sxz = C.x, syz = C.y;
-                const float r2 = dx * dx + dy * dy + dz * dz;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                 const float ri = rsqrtf(r2);
                 const float ri2 = ri * ri, ri3 = ri2 * ri, ri5 = ri3 * ri2;
-                const float sdx = sxx * dx + sxy * dy + sxz * dz;
-                const float sdy = sxy * dx + syy * dy + syz * dz;
-                const float sdz = sxz * dx + syz * dy + szz * dz;
-                const float dsd = dx * sdx + dy * sdy + dz * sdz;
-                const float tr = sxx + syy + szz;
-                // a = M d/r^3 - 3 S d/r^5 + 7.5 (d.S.d) d/r^7 - 1.5 tr(S) d/r^5
-                const float cd = M * ri3 + (7.5f * dsd * ri2 - 1.5f * tr) * ri5;
-                ax += cd * dx - 3.f * ri5 * sdx;
-                ay += cd * dy - 3.f * ri5 * sdy;
-                az += cd * dz - 3.f * ri5 * sdz;
-                // phi = -M/r - 1.5 (d.S.d)/r^5 + 0.5 tr(S)/r^3
-                pot += -M * ri - 1.5f * dsd * ri5 + 0.5f * tr * ri3;
+                // Q d with B = (Qxx, Qyy, Qzz, Qxy), C = (Qxz, Qyz)
+                const float qx = fmaf(C.x, dz, fmaf(B.w, dy, B.x * dx));
+                const float qy = fmaf(C.y, dz, fmaf(B.y, dy, B.w * dx));
+                const float qz = fmaf(B.z, dz, fmaf(C.y, dy, C.x * dx));
+                const float dqd = fmaf(dz, qz, fmaf(dy, qy, dx * qx));
+                const float c = fmaf(2.5f * dqd, ri2 * ri5, A.w * ri3);
+                ax = fmaf(c, dx, ax);
+                ay = fmaf(c, dy, ay);
+                az = fmaf(c, dz, az);
+                sx = fmaf(ri5, qx, sx);
+                sy = fmaf(ri5, qy, sy);
+                sz = fmaf(ri5, qz, sz);
+                pm = fmaf(A.w, ri, pm);
+                pq = fmaf(dqd, ri5, pq);
             }
-            fx += ax;
-            fy += ay;
-            fz += az;
-            fp += pot;
+            fx += (double)(ax - sx);
+            fy += (double)(ay - sy);
+            fz += (double)(az - sz);
+            fp -= (double)(pm + 0.5f * pq);
             ncell = 0;
             __syncwarp();
         };
@@ -416,19 +422,19 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
             for (int e = 0; e < nfar; e++) {
                 const float4 P = fl[e];
                 const float dx = P.x - xi, dy = P.y - yi, dz = P.z - zi;
-                const float r2 = dx * dx + dy * dy + dz * dz;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                 const float ri = rsqrtf(r2);
                 const float mr = P.w * ri;
                 const float mr3 = mr * ri * ri;
-                ax += mr3 * dx;
-                ay += mr3 * dy;
-                az += mr3 * dz;
-                pot -= mr;
+                ax = fmaf(mr3, dx, ax);
+                ay = fmaf(mr3, dy, ay);
+                az = fmaf(mr3, dz, az);
+                pot += mr;
             }
             fx += ax;
             fy += ay;
             fz += az;
-            fp += pot;
+            fp -= pot;
             nfar = 0;
             __syncwarp();
         };
@@ -530,8 +536,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
                 const NodeMP P = a.mp[node];
                 cl[0][p] = make_float4((float)(P.mx - cx), (float)(P.my - cy), (float)(P.mz - cz),
                                        (float)P.m);
-                cl[1][p] = make_float4(P.s[0], P.s[1], P.s[2], P.s[3]);
-                cl[2][p] = make_float4(P.s[4], P.s[5], 0.f, 0.f);
+                cl[1][p] = make_float4(P.q[0], P.q[1], P.q[2], P.q[3]);
+                cl[2][p] = make_float4(P.q[4], P.q[5], 0.f, 0.f);
             }
             ncell += __popc(cm);
             __syncwarp();
