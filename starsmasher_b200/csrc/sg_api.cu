@@ -189,7 +189,7 @@ struct sphgrav_ctx {
     DBuf<int> tcnt, toff, tstack, tgcount, theavy;
     DBuf<double> theavy_part, tacc;
     DBuf<unsigned char> tgflag;
-    DBuf<int2> tglist;
+    DBuf<int2> tglist, tgorder;
     DBuf<unsigned char> tscan;
     DBuf<double> tres, twsum;
     DBuf<float> probe_sink;
@@ -575,6 +575,11 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     int ngroups = 0;
     CUDA_TRY(cudaMemcpyAsync(&ngroups, c->tgcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
+    // walking order: largest H first (the build's scratch holds the sort keys)
+    TRY(ensure(c, c->tgorder, (size_t)std::max(ngroups, 1), "tree groups"));
+    TRY(ensure(c, c->tscan, tree_order_temp_bytes(ngroups), "tree scan"));
+    CUDA_TRY(tree_order_groups(ngroups, c->tglist.p, c->tgorder.p, D.h2, (unsigned *)c->tcnt.p,
+                               (unsigned *)c->toff.p, c->tscan.p, c->tscan.cap, st));
     TRY(ensure(c, c->tgeom, (size_t)nn, "tree geometry"));
     TRY(ensure(c, c->tmp, (size_t)nn, "tree multipoles"));
     TRY(ensure(c, c->tacc, tree_acc_bytes(nn) / sizeof(double), "tree node sums"));
@@ -590,7 +595,7 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     a.D = D;
     a.n = n;
     a.ngroups = ngroups;
-    a.groups = c->tglist.p;
+    a.groups = c->tgorder.p;
     TRY(ensure(c, c->theavy, (size_t)std::max(ngroups, 1), "tree heavy groups"));
     CUDA_TRY(cudaMemsetAsync(c->tgcount.p + 1, 0, sizeof(int), st));
     a.heavy = c->theavy.p;
@@ -619,7 +624,7 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     if (nheavy > 0) {
         TRY(ensure(c, c->theavy_part, (size_t)nheavy * tree_heavy_chunks(nheavy, n) * 4 * 32,
                    "tree heavy sums"));
-        CUDA_TRY(tree_heavy(nheavy, c->theavy.p, c->tglist.p, D, n, nkernel, c->theavy_part.p,
+        CUDA_TRY(tree_heavy(nheavy, c->theavy.p, c->tgorder.p, D, n, nkernel, c->theavy_part.p,
                             c->tres.p, st));
     }
     c->tree_groups_last = ngroups;
@@ -929,6 +934,7 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release();
     c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();
     c->twsum.release(); c->tgcount.release(); c->tgflag.release(); c->tglist.release();
+    c->tgorder.release();
     c->theavy.release(); c->theavy_part.release(); c->tacc.release();
     c->h_in.release(); c->h_out.release(); c->h_err.release();
     for (auto &e : c->prof_events) {

@@ -163,6 +163,11 @@ cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, int *lev
 // Lists the walking groups (order not significant); *ngroups via `count`.
 cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag, int2 *glist,
                         int *count, cudaStream_t st);
+// Groups sorted by descending largest H^2 of their particles (walking order).
+size_t tree_order_temp_bytes(int ng);
+cudaError_t tree_order_groups(int ng, const int2 *glist, int2 *ordered, const double *h2,
+                              unsigned *keys_in, unsigned *keys_out, void *temp, size_t temp_bytes,
+                              cudaStream_t st);
 // Node properties; acc_buf: tree_acc_bytes(nn) of scratch.
 size_t tree_acc_bytes(int nn);
 cudaError_t tree_props(int nn, const TreeNode *nodes, const SortedF64 &D, double theta,

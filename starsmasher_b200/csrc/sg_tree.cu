@@ -28,6 +28,7 @@
 // reduction has a fixed order: results are bit-for-bit reproducible.
 #include "sg_launch.h"
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
         //   a = M d/r^3 - Q d/r^5 + 2.5 (d.Q.d) d/r^7,  phi = -M/r - 0.5 (d.Q.d)/r^5
         auto eval_cells = [&]() {
             float ax = 0.f, ay = 0.f, az = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, pm = 0.f, pq = 0.f;
+#pragma unroll 2  // measured: -15% walk time at theta 0.5, N = 1M (with the far loop's 4)
             for (int e = 0; e < ncell; e++) {
                 const float4 A = cl[0][e], B = cl[1][e], C = cl[2][e];
                 const float dx = A.x - xi, dy = A.y - yi, dz = A.z - zi;
@@ -419,6 +421,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
         // Far particles: Newtonian FP32 pairs, no per-pair test (r > 0 as above).
         auto eval_far = [&]() {
             float ax = 0.f, ay = 0.f, az = 0.f, pot = 0.f;
+#pragma unroll 4
             for (int e = 0; e < nfar; e++) {
                 const float4 P = fl[e];
                 const float dx = P.x - xi, dy = P.y - yi, dz = P.z - zi;
@@ -784,6 +787,43 @@ cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gfla
     k_tree_groups<<<std::min((nn + 255) / 256, 4096), 256, 0, st>>>(nn, nodes, gflag, glist, count);
     ++g_launches;
     return cudaGetLastError();
+}
+
+// Walking order: the largest H first.  Every particle within H of a group
+// is tested pair by pair, so those groups walk longest; started first, they
+// do not leave one warp running after the rest (results do not depend on the
+// order: each group's sums are its own).
+__global__ void k_tree_group_keys(int ng, const int2 *glist, const double *h2, unsigned *keys)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ng) return;
+    const int2 r = glist[g];
+    double m = 0.0;
+    for (int s = r.x; s < r.y; s++) m = fmax(m, h2[s]);
+    keys[g] = __float_as_uint((float)m);  // non-negative floats order as their bits
+}
+
+size_t tree_order_temp_bytes(int ng)
+{
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const unsigned *)nullptr,
+                                              (unsigned *)nullptr, (const int2 *)nullptr,
+                                              (int2 *)nullptr, ng);
+    return bytes;
+}
+
+cudaError_t tree_order_groups(int ng, const int2 *glist, int2 *ordered, const double *h2,
+                              unsigned *keys_in, unsigned *keys_out, void *temp, size_t temp_bytes,
+                              cudaStream_t st)
+{
+    if (ng <= 0) return cudaSuccess;
+    k_tree_group_keys<<<(ng + 255) / 256, 256, 0, st>>>(ng, glist, h2, keys_in);
+    ++g_launches;
+    size_t tb = temp_bytes;
+    const cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(temp, tb, keys_in, keys_out,
+                                                                    glist, ordered, ng, 0, 32, st);
+    ++g_launches;
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 size_t tree_acc_bytes(int nn) { return (size_t)nn * sizeof(NodeAcc); }
