@@ -10,10 +10,17 @@ Reference behaviour restated:
     with mpi_gatherv, balAV3.f:423-434, and allreduces accelerations,
     balAV3.f:478-483; here each rank's rows are all-gathered);
   * independent particle sets (batches) are sharded whole, longest first by
-    pair count, with no data exchange before the gather.
+    pair count, with no data exchange before the gather;
+  * device-resident form (``forces_row_split_device``): every rank holds the
+    positions of its own rows (as after the reference's integrator step), the
+    five source arrays are all-gathered on the device (NCCL over NVLink), each
+    rank evaluates its rows against all n sources, and the row slices are
+    all-gathered again; no reduction is needed.
 
-The per-rank computation is a callable, so the same logic runs with the GPU
-library (``gpu_compute``) or, in the CPU tests, with any other evaluator.
+Collective buffers live on the process group's device: the current CUDA
+device under NCCL, host memory under gloo.  The per-rank computation is a
+callable, so the same logic runs with the GPU library (``gpu_compute``,
+``gpu_compute_device``) or, in the CPU tests, with any other evaluator.
 """
 from __future__ import annotations
 
@@ -45,19 +52,40 @@ def shard_sets(sizes: Sequence[int], nranks: int) -> List[List[int]]:
     return [sorted(v) for v in out]
 
 
-def _allgather_rows(group, rank: int, nranks: int, n: int, lo: int, part: np.ndarray):
+def comm_device(group=None):
+    """Where collective buffers must live for ``group``: NCCL takes CUDA
+    tensors (the current device), gloo host tensors."""
     import torch
     import torch.distributed as dist
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def allgather_rows(part, n: int, group=None):
+    """All-gather row slices: ``part`` is a (k, hi - lo) tensor holding this
+    rank's rows [lo, hi) of gpu_row_range; returns the (k, n) tensor on
+    ``part``'s device.  Slices are padded to the common stride (all_gather
+    wants equal sizes) and unpadded on arrival."""
+    import torch
+    import torch.distributed as dist
+    nranks = dist.get_world_size(group)
     stride = (n - 1) // nranks + 1 if n > 0 else 0
-    buf = torch.zeros((4, stride), dtype=torch.float64)
-    buf[:, : part.shape[1]] = torch.from_numpy(part)
-    bufs = [torch.zeros_like(buf) for _ in range(nranks)]
+    buf = part.new_zeros((part.shape[0], stride))
+    buf[:, : part.shape[1]] = part
+    bufs = [torch.empty_like(buf) for _ in range(nranks)]
     dist.all_gather(bufs, buf, group=group)
-    full = np.zeros((4, n))
+    full = part.new_empty((part.shape[0], n))
     for r in range(nranks):
         a, b = gpu_row_range(n, nranks, r)
-        full[:, a:b] = bufs[r].numpy()[:, : b - a]
+        full[:, a:b] = bufs[r][:, : b - a]
     return full
+
+
+def _allgather_rows(group, rank: int, nranks: int, n: int, lo: int, part: np.ndarray):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(part)).to(comm_device(group))
+    return allgather_rows(t, n, group).cpu().numpy()
 
 
 def forces_row_split(compute: RowCompute, x, y, z, m, range2, group=None):
@@ -92,9 +120,9 @@ def forces_set_shard(compute: RowCompute, offsets, x, y, z, m, range2, group=Non
         for q in range(4):
             local[q, a:b] = np.asarray(res[q])[: b - a]
         owned[a:b] = 1.0
-    t = torch.from_numpy(np.vstack([local, owned[None, :]]))
+    t = torch.from_numpy(np.vstack([local, owned[None, :]])).to(comm_device(group))
     dist.all_reduce(t, group=group)  # each row is owned by exactly one rank
-    t = t.numpy()
+    t = t.cpu().numpy()
     assert np.all(t[4] == 1.0)
     return tuple(t[q].copy() for q in range(4))
 
@@ -103,4 +131,44 @@ def gpu_compute(ctx, nkernel: int = 0, precision: str = "f32split") -> RowComput
     """Per-rank computation with the GPU library (host arrays)."""
     def f(x, y, z, m, range2, i_begin, ni):
         return ctx.forces(x, y, z, m, range2, nkernel, precision, i_begin, ni)
+    return f
+
+
+# compute(src, i_begin, ni, out): src a (5, n) tensor of x, y, z, m, range2;
+# fills rows [i_begin, i_begin + ni) of the (4, n) tensor out (ax, ay, az, pot)
+DeviceRowCompute = Callable[[object, int, int, object], None]
+
+
+def forces_row_split_device(compute: DeviceRowCompute, own, n: int, group=None):
+    """Device-resident row split of one set.  ``own`` is the (5, hi - lo)
+    tensor of this rank's rows [lo, hi) (x, y, z, m, range2); the sources are
+    all-gathered, the rank's rows evaluated against all n of them, and the
+    (4, n) result all-gathered, every tensor on ``own``'s device.  Returns
+    (sources, result)."""
+    import torch.distributed as dist
+    nranks = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    lo, hi = gpu_row_range(n, nranks, rank)
+    if own.shape[1] != hi - lo:
+        raise ValueError(f"rank {rank} holds {own.shape[1]} rows, its slice is {hi - lo}")
+    src = allgather_rows(own, n, group)
+    out = src.new_zeros((4, n))
+    compute(src, lo, hi - lo, out)
+    return src, allgather_rows(out[:, lo:hi], n, group)
+
+
+def gpu_compute_device(ctx, nkernel: int = 0, precision: str = "f32split") -> DeviceRowCompute:
+    """Per-rank computation with the GPU library on device tensors.  The
+    library runs on the context's stream: torch's stream (where the gathered
+    sources and the zeroed outputs were written) is drained first, and the
+    call returns after the library finished, so the collective that follows
+    sees the rows."""
+    import torch
+
+    def f(src, i_begin, ni, out):
+        torch.cuda.current_stream(src.device).synchronize()
+        n = src.shape[1]
+        ctx.forces_device(n, src[0], src[1], src[2], src[3], src[4], out[0], out[1], out[2],
+                          out[3], nkernel=nkernel, precision=precision, i_begin=i_begin, ni=ni)
+        ctx.sync()
     return f

@@ -76,6 +76,57 @@ def test_two_rank_split_equals_single(mode):
             np.testing.assert_array_equal(a, r)
 
 
+def _oracle_compute_tensor(src, i_begin, ni, out):
+    import torch
+    a = [src[q].numpy() for q in range(5)]
+    r = _oracle_compute(*a, i_begin, ni)
+    for q in range(4):
+        out[q, i_begin:i_begin + ni] = torch.from_numpy(np.asarray(r[q]))
+
+
+def _worker_device(rank, world, port, q):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        s = inputs.single_polytrope(701, 1.5, seed=3)
+        lo, hi = multirank.gpu_row_range(s.n, world, rank)
+        own = torch.from_numpy(np.stack([a[lo:hi] for a in (s.x, s.y, s.z, s.m, s.range2)]))
+        src, res = multirank.forces_row_split_device(_oracle_compute_tensor, own, s.n)
+        q.put((rank, src.numpy(), res.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_device_form_gathers_sources_and_rows():
+    """The device-resident form on gloo host tensors: each rank starts with
+    only its own rows' positions; sources and results are all-gathered."""
+    import oracle
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_device, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = {r: (src, res) for r, src, res in (q.get(timeout=120) for _ in range(2))}
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    s = inputs.single_polytrope(701, 1.5, seed=3)
+    ref = oracle.rows(s.x, s.y, s.z, s.m, s.range2, 0)
+    for rank in (0, 1):
+        src, res = got[rank]
+        for qd, a in enumerate((s.x, s.y, s.z, s.m, s.range2)):
+            np.testing.assert_array_equal(src[qd], a)
+        for qd in range(4):
+            np.testing.assert_array_equal(res[qd], ref[qd])
+
+
 def test_row_ranges_and_set_shards():
     assert multirank.gpu_row_range(1001, 4, 3) == (753, 1001)
     assert [multirank.gpu_row_range(10, 3, r) for r in range(3)] == [(0, 4), (4, 8), (8, 10)]
