@@ -5,27 +5,33 @@
 //   * an octree over the Morton-sorted particles; a node splits while it
 //     holds more than TREE_LEAF particles (the reference: 64);
 //   * every node carries its mass, centre of mass and second moment about
-//     it (monopole + quadrupole, as libSequoia's body_node);
-//   * particles are walked in groups, one warp each: the largest nodes that
-//     hold at most 32 particles (a leaf that cannot split is cut into chunks
-//     of 32); a node is opened when the gap between the group's and the
-//     node's bounding boxes is at most l / theta, l the node's edge length
-//     (libSequoia's minimum-distance criterion, compute_properties.cu:339,
-//     dev_shared_traverse_functions.cu:311-337); theta comes from
-//     gpu_init_dev_ (main.f:269-270 passes 0.3).  It is also opened when the
-//     gap is at most max(H) of the node's or the group's particles, so every
-//     pair closer than the softening length is evaluated particle by
-//     particle with the softened kernel (the reference leaves that test out,
-//     INDSOFT); with theta -> 0 the walk is therefore the direct sum;
-//   * accepted nodes interact through the quadrupole expansion, opened
-//     leaves particle by particle: FP32 for Newtonian pairs, FP64 with the
+//     it (monopole + quadrupole, as libSequoia's body_node), built bottom-up
+//     in FP64; the walk uses the traceless quadrupole 3S - tr(S)I;
+//   * particles are walked in groups, one warp each: the children of every
+//     node with more than 32 particles, consecutive small siblings merged up
+//     to 32 (a leaf that cannot split is cut into chunks of 32), the groups
+//     with the largest H first; a node is opened when the gap between the
+//     group's and the node's bounding boxes is at most l / theta, l the
+//     node's edge length (libSequoia's minimum-distance criterion,
+//     compute_properties.cu:339, dev_shared_traverse_functions.cu:311-337);
+//     theta comes from gpu_init_dev_ (main.f:269-270 passes 0.3).  It is
+//     also opened when the gap is at most max(H) of the node's or the
+//     group's particles, so every pair closer than the softening length is
+//     evaluated particle by particle with the softened kernel (the reference
+//     leaves that test out, INDSOFT); with theta -> 0 the walk is therefore
+//     the direct sum;
+//   * accepted nodes interact through the quadrupole expansion in FP32;
+//     particles of opened leaves that lie farther than every H from the
+//     group's box are Newtonian FP32 pairs without a per-pair test, the
+//     others are tested pair by pair: FP32 when Newtonian, FP64 with the
 //     CPU-path formulas (pair_f64_core) for r < max(H_i, H_j) and r = 0;
-//   * a group with more than TREE_BUDGET particles within the largest H of
-//     its box (a dense region inside a softening sphere, e.g. a point-mass
-//     core with a large H) leaves the walk and gets the direct FP64 sum over
-//     all particles instead, spread over many CTAs (k_tree_heavy).
-// Construction is level by level with prefix sums (no atomics), and every
-// reduction has a fixed order: results are bit-for-bit reproducible.
+//   * a group with more than TREE_BUDGET tested particles (a dense region
+//     inside a softening sphere, e.g. a point-mass core with a large H)
+//     leaves the walk and gets the direct FP64 sum over all particles
+//     instead, spread over many CTAs (k_tree_heavy).
+// Construction is level by level with prefix sums.  Atomics only order the
+// group list and hand groups to warps; every sum has a fixed order, so the
+// results are bit-for-bit reproducible.
 #include "sg_launch.h"
 
 #include <cub/device/device_radix_sort.cuh>
