@@ -13,7 +13,7 @@ module sphgrav_b200_mod
   implicit none
 
   integer(c_int), parameter :: SPHGRAV_OK = 0
-  integer(c_int), parameter :: SPHGRAV_FP64 = 0, SPHGRAV_F32SPLIT = 1
+  integer(c_int), parameter :: SPHGRAV_FP64 = 0, SPHGRAV_F32SPLIT = 1, SPHGRAV_TREE = 2
 
   interface
     integer(c_int) function sphgrav_create(ctx, device) bind(C, name="sphgrav_create")
@@ -79,6 +79,22 @@ module sphgrav_b200_mod
                                               bind(C, name="sphgrav_legacy_set_precision")
       import :: c_int
       integer(c_int), value :: precision
+    end function
+
+    ! SPHGRAV_TREE: opening angle in [0, 2] (gpu_init_dev_'s theta sets the
+    ! legacy calls' angle)
+    integer(c_int) function sphgrav_set_theta(ctx, theta) bind(C, name="sphgrav_set_theta")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: theta
+    end function
+
+    ! SPHGRAV_TREE: walking groups of the last call, and those handed to the
+    ! direct FP64 sum
+    integer(c_int) function sphgrav_tree_stats(ctx, groups, heavy) bind(C, name="sphgrav_tree_stats")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), intent(out) :: groups, heavy
     end function
 
     type(c_ptr) function sphgrav_last_error_message() bind(C, name="sphgrav_last_error_message")

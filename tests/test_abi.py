@@ -40,6 +40,23 @@ def test_python_binding_covers_the_header():
     assert set(declared_functions()) == set(_lib.SIGNATURES)
 
 
+def test_fortran_module_binds_declared_symbols():
+    """Every bind(C) name of the Fortran interface module is a declared,
+    exported symbol, and its precision constants match the header's enum (no
+    Fortran compiler here: the module is checked as text)."""
+    f90 = open(os.path.join(ROOT, "starsmasher_b200", "fortran", "sphgrav_b200_mod.f90")).read()
+    bound = re.findall(r'bind\(C,\s*name="(\w+)"\)', f90)
+    assert len(bound) >= 10
+    declared = set(declared_functions())
+    for name in bound:
+        assert name in declared, name
+    hdr = open(HEADER).read()
+    for const in ("SPHGRAV_FP64", "SPHGRAV_F32SPLIT", "SPHGRAV_TREE"):
+        want = re.search(rf"{const}\s*=\s*(\d+)", hdr).group(1)
+        got = re.search(rf"{const}\s*=\s*(\d+)", f90).group(1)
+        assert got == want, const
+
+
 def test_static_archive_for_fortran_link():
     a = os.path.join(os.path.dirname(_lib.LIB_PATH), "libSPHgrav.a")
     assert os.path.exists(a)
