@@ -89,7 +89,7 @@ def test_gravforce_host_mirror_matches(gpu_ctx):
     assert r["acc_max"] <= FP64_TOL and r["pot_max"] <= FP64_TOL
 
 
-@pytest.mark.parametrize("precision", ["fp64", "f32split"])
+@pytest.mark.parametrize("precision", ["fp64", "f32split", "tree"])
 def test_gravforce_device_matches_host_mirror(gpu_ctx, precision):
     """sphgrav_gravforce_device (positions, hp, u on the device; range2 built
     there) gives the host mirror's rows bit for bit and leaves the others."""

@@ -109,6 +109,19 @@ def test_heavy_group_is_exact(gpu_ctx):
         assert np.array_equal(u, v)
 
 
+@pytest.mark.parametrize("case", ["3stars_start1", "collision_start1"])
+def test_reference_snapshot_potential(gpu_ctx, case):
+    """The potentials the reference stored in its own dumps (grpot of
+    sph.start1u, written by its gravity code) against the tree at the
+    reference's theta = 0.3: RMS <= 1e-4, max <= 1e-3 relative."""
+    from conftest import load_golden
+    d = load_golden(case)
+    gpu_ctx.set_theta(0.3)
+    got = gpu_ctx.forces(d["x"], d["y"], d["z"], d["am"], d["range2"], 0, "tree")
+    rel = np.abs(got[3] - d["grpot"]) / np.abs(d["grpot"])
+    assert np.sqrt(np.mean(rel ** 2)) <= 1e-4 and rel.max() <= 1e-3, (rel.max(), np.sqrt(np.mean(rel ** 2)))
+
+
 def test_energy_per_set(gpu_ctx, star16k):
     t = _torch()
     s = star16k
