@@ -186,7 +186,7 @@ struct sphgrav_ctx {
     DBuf<TreeNode> tnodes;
     DBuf<NodeGeom> tgeom;
     DBuf<NodeMP> tmp;
-    DBuf<int> tcnt, toff, tstack, tgcount, theavy;
+    DBuf<int> tcnt, toff, tstack, tgcount, theavy, tlv;
     DBuf<double> theavy_part, tacc;
     DBuf<unsigned char> tgflag;
     DBuf<int2> tglist, tgorder;
@@ -546,8 +546,16 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     TRY(ensure(c, c->toff, (size_t)n + 1, "tree scratch"));
     TRY(ensure(c, c->tscan, tree_scan_temp_bytes(n + 1), "tree scan"));
     TRY(ensure(c, c->tnodes, std::max<size_t>(c->tnodes.cap, 2 * (size_t)n + 64), "tree nodes"));
+    // walking groups: runs of sibling nodes with <= TREE_GROUP particles
+    TRY(ensure(c, c->tglist, (size_t)n, "tree groups"));
+    TRY(ensure(c, c->tgcount, 2, "tree groups"));  // [0] groups, [1] heavy groups
+    TRY(ensure(c, c->tlv, TREE_LV_SIZE, "tree levels"));
+    // The build is issued TREE_BATCH levels at a time; one read-back of the
+    // level table per batch shows whether the tree has ended (an empty level)
+    // or the node array is full (it is regrown and the build repeated).
+    constexpr int TREE_BATCH = 4;
+    int lvh[TREE_LV_SIZE];
     int nn = 0, depth = 0;
-    int level_start[TREE_LEVELS + 2];
     for (;;) {
         TRY(ensure(c, c->tgflag, c->tnodes.cap, "tree groups"));
         TreeBuildArgs t;
@@ -560,21 +568,27 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
         t.scan_temp = c->tscan.p;
         t.scan_temp_bytes = c->tscan.cap;
         t.gflag = c->tgflag.p;
-        const cudaError_t e = tree_build(t, &nn, &depth, level_start, st);
-        if (e == cudaErrorMemoryAllocation) {
-            TRY(ensure(c, c->tnodes, 2 * c->tnodes.cap, "tree nodes"));
-            continue;
+        t.lv = c->tlv.p;
+        bool overflow = false;
+        for (int l0 = 0; l0 < TREE_LEVELS; l0 += TREE_BATCH) {
+            const int l1 = std::min(l0 + TREE_BATCH, TREE_LEVELS);
+            CUDA_TRY(tree_build_levels(t, l0, l1, st));
+            CUDA_TRY(cudaMemcpyAsync(lvh, c->tlv.p, sizeof(lvh), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            overflow = lvh[TREE_LV_OVERFLOW] != 0;
+            nn = lvh[l1 + 1];  // end of level l1, the last one written
+            depth = l1;
+            if (overflow || lvh[l1 + 1] == lvh[l1]) break;  // level l1 is empty
         }
-        CUDA_TRY(e);
-        break;
+        if (!overflow) break;
+        TRY(ensure(c, c->tnodes, 2 * c->tnodes.cap, "tree nodes"));
     }
-    // walking groups: maximal nodes with <= TREE_GROUP particles
-    TRY(ensure(c, c->tglist, (size_t)n, "tree groups"));
-    TRY(ensure(c, c->tgcount, 2, "tree groups"));  // [0] groups, [1] heavy groups
+    while (depth > 0 && lvh[depth + 1] == lvh[depth]) depth--;  // deepest non-empty level
     CUDA_TRY(tree_groups(nn, c->tnodes.p, c->tgflag.p, c->tglist.p, c->tgcount.p, st));
     int ngroups = 0;
     CUDA_TRY(cudaMemcpyAsync(&ngroups, c->tgcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
+    const int *level_start = lvh;
     // walking order: largest H first (the build's scratch holds the sort keys)
     TRY(ensure(c, c->tgorder, (size_t)std::max(ngroups, 1), "tree groups"));
     TRY(ensure(c, c->tscan, tree_order_temp_bytes(ngroups), "tree scan"));
@@ -934,7 +948,7 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release();
     c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();
     c->twsum.release(); c->tgcount.release(); c->tgflag.release(); c->tglist.release();
-    c->tgorder.release();
+    c->tgorder.release(); c->tlv.release();
     c->theavy.release(); c->theavy_part.release(); c->tacc.release();
     c->h_in.release(); c->h_out.release(); c->h_err.release();
     for (auto &e : c->prof_events) {

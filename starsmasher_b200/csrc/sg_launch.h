@@ -95,6 +95,10 @@ cudaError_t launch_wait_selftest(uint32_t polls, int *err, cudaStream_t st);
 // --- Barnes-Hut octree (sg_tree.cu)
 constexpr int TREE_LEAF = 16;    // a node with more particles splits
 constexpr int TREE_LEVELS = 21;  // Morton bits per axis
+// device level table: [L] first node of level L (L = 0..TREE_LEVELS + 1), then a
+// node-capacity overflow flag
+constexpr int TREE_LV_OVERFLOW = TREE_LEVELS + 2;
+constexpr int TREE_LV_SIZE = TREE_LEVELS + 3;
 constexpr int TREE_STACK = 8192; // traversal stack entries per warp
 constexpr int TREE_GROUP = 32;   // a walking group: a maximal node with <= 32 particles
 constexpr int TREE_BUDGET = 8192;  // particles within the largest H of a group's box (each
@@ -135,6 +139,7 @@ struct TreeBuildArgs {
     int cap;                         // node capacity
     int *cnt, *off;                  // per-level scratch (n + 1 entries)
     unsigned char *gflag;            // per node: a walking group (maximal with <= TREE_GROUP)
+    int *lv;                         // device level table (TREE_LV_SIZE ints)
     void *scan_temp;
     size_t scan_temp_bytes;
 };
@@ -156,10 +161,11 @@ struct TreeWalkArgs {
 size_t tree_scan_temp_bytes(int n);
 // Builds the octree; returns cudaErrorMemoryAllocation (nothing else
 // changed) when `cap` nodes do not suffice.  Synchronises once per level.
-// level_start: TREE_LEVELS + 2 entries; nodes of level l are [level_start[l], level_start[l + 1]),
-// levels 0..depth.
-cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, int *level_start,
-                       cudaStream_t st);
+// Issues levels [level_begin, level_end) without a host wait (level 0 also
+// sets up the root); t.lv receives the level table (nodes of level l are
+// [lv[l], lv[l + 1])) and the overflow flag.
+cudaError_t tree_build_levels(const TreeBuildArgs &t, int level_begin, int level_end,
+                              cudaStream_t st);
 // Lists the walking groups (order not significant); *ngroups via `count`.
 cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag, int2 *glist,
                         int *count, cudaStream_t st);

@@ -67,30 +67,51 @@ __device__ __forceinline__ void child_bounds(const TreeNode &T, int level,
         b[d] = lower_bound_key(keys, b[d - 1], T.end, base | ((unsigned long long)d << sh));
 }
 
-__global__ void k_tree_count(int l0, int l1, int level, const TreeNode *nodes,
+// Level bounds live on the device (lv[L] = first node of level L, lv[L + 1]
+// its end; lv[TREE_LV_OVERFLOW] set when the node array is too small), so the
+// host issues every level without waiting.  Level L has at most `bound`
+// nodes (min(8^L, n)); counts are written for the whole bound, zero past the
+// level's end, so that one fixed-size scan gives the child offsets.
+__global__ void k_tree_count(int level, int bound, const int *lv, const TreeNode *nodes,
                              const unsigned long long *keys, int *cnt)
 {
-    const int i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= l1) return;
-    const TreeNode T = nodes[i];
-    int c = 0;
-    if (T.end - T.start > TREE_LEAF && level < TREE_LEVELS) {
-        int b[9];
-        child_bounds(T, level, keys, b);
-        for (int d = 0; d < 8; d++) c += b[d + 1] > b[d] ? 1 : 0;
+    const int l0 = lv[level], l1 = lv[level + 1];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < bound; j += gridDim.x * blockDim.x) {
+        const int i = l0 + j;
+        int c = 0;
+        if (i < l1) {
+            const TreeNode T = nodes[i];
+            if (T.end - T.start > TREE_LEAF && level < TREE_LEVELS) {
+                int b[9];
+                child_bounds(T, level, keys, b);
+                for (int d = 0; d < 8; d++) c += b[d + 1] > b[d] ? 1 : 0;
+            }
+        }
+        cnt[j] = c;
     }
-    cnt[i - l0] = c;
 }
 
-__global__ void k_tree_emit(int l0, int l1, int level, TreeNode *nodes,
-                            const unsigned long long *keys, const int *cnt, const int *off,
-                            int next_base, unsigned char *gflag)
+// One thread: the end of level + 1 from the scan; past the capacity the
+// overflow flag is set and the tree stops at this level.
+__global__ void k_tree_next(int level, int cap, int *lv, const int *cnt, const int *off)
 {
-    const int i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= l1) return;
+    const int count = lv[level + 1] - lv[level];
+    const long long total = count > 0 ? (long long)off[count - 1] + cnt[count - 1] : 0;
+    if (lv[level + 1] + total > cap) {
+        lv[TREE_LV_OVERFLOW] = 1;
+        lv[level + 2] = lv[level + 1];
+    } else {
+        lv[level + 2] = lv[level + 1] + (int)total;
+    }
+}
+
+__device__ void emit_children(int i, int l0, int level, int next_base, TreeNode *nodes,
+                              const unsigned long long *keys, const int *cnt, const int *off,
+                              unsigned char *gflag)
+{
     const int c = cnt[i - l0];
-    TreeNode T = nodes[i];
     if (c == 0) return;
+    TreeNode T = nodes[i];
     int b[9];
     child_bounds(T, level, keys, b);
     int k = next_base + off[i - l0];
@@ -131,6 +152,17 @@ __global__ void k_tree_emit(int l0, int l1, int level, TreeNode *nodes,
     if (run >= 0) gflag[run] = (unsigned char)run_len;
 }
 
+__global__ void k_tree_emit(int level, const int *lv, TreeNode *nodes,
+                            const unsigned long long *keys, const int *cnt, const int *off,
+                            unsigned char *gflag)
+{
+    const int l0 = lv[level], l1 = lv[level + 1];
+    if (lv[level + 2] == l1) return;  // no children (or no room: overflow is flagged)
+    for (int i = l0 + blockIdx.x * blockDim.x + threadIdx.x; i < l1;
+         i += gridDim.x * blockDim.x)
+        emit_children(i, l0, level, l1, nodes, keys, cnt, off, gflag);
+}
+
 // Walking groups: runs of consecutive sibling nodes that together hold at
 // most TREE_GROUP particles (each a maximal such node or merged with its
 // neighbours), and TREE_GROUP-particle chunks of the (coincident-particle)
@@ -150,8 +182,11 @@ __global__ void k_tree_groups(int nn, const TreeNode *nodes, const unsigned char
     }
 }
 
-__global__ void k_tree_root(TreeNode *nodes, int n, unsigned char *gflag)
+__global__ void k_tree_root(TreeNode *nodes, int n, unsigned char *gflag, int *lv)
 {
+    lv[0] = 0;
+    lv[1] = 1;
+    lv[TREE_LV_OVERFLOW] = 0;
     gflag[0] = n <= TREE_GROUP;
     TreeNode R;
     R.start = 0;
@@ -747,41 +782,28 @@ size_t tree_scan_temp_bytes(int n)
     return b;
 }
 
-cudaError_t tree_build(const TreeBuildArgs &t, int *nnodes, int *depth, int *level_start,
-                       cudaStream_t st)
+cudaError_t tree_build_levels(const TreeBuildArgs &t, int level_begin, int level_end,
+                              cudaStream_t st)
 {
-    cudaError_t e;
-    k_tree_root<<<1, 1, 0, st>>>(t.nodes, t.n, t.gflag);
-    ++g_launches;
-    int l0 = 0, l1 = 1, level = 0;
-    while (l1 > l0) {
-        level_start[level] = l0;
-        const int cnt_n = l1 - l0;
-        const int blocks = (cnt_n + 255) / 256;
-        k_tree_count<<<blocks, 256, 0, st>>>(l0, l1, level, t.nodes, t.keys, t.cnt);
+    if (level_begin == 0) {
+        k_tree_root<<<1, 1, 0, st>>>(t.nodes, t.n, t.gflag, t.lv);
+        ++g_launches;
+    }
+    for (int level = level_begin; level < level_end; level++) {
+        // level has at most min(8^level, n) nodes
+        const int bound = (int)std::min<long long>(1ll << (3 * level), (long long)std::max(t.n, 1));
+        const int blocks = std::min((bound + 255) / 256, 4096);
+        k_tree_count<<<blocks, 256, 0, st>>>(level, bound, t.lv, t.nodes, t.keys, t.cnt);
         ++g_launches;
         size_t tb = t.scan_temp_bytes;
-        if ((e = cub::DeviceScan::ExclusiveSum(t.scan_temp, tb, t.cnt, t.off, cnt_n, st)) != cudaSuccess)
-            return e;
-        // children of this level = off[last] + cnt[last]
-        int tail[2];
-        if ((e = cudaMemcpyAsync(&tail[0], t.off + cnt_n - 1, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-            return e;
-        if ((e = cudaMemcpyAsync(&tail[1], t.cnt + cnt_n - 1, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-            return e;
-        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-        const int nchild = tail[0] + tail[1];
-        if (nchild == 0) break;
-        if ((long long)l1 + nchild > t.cap) return cudaErrorMemoryAllocation;  // caller grows and retries
-        k_tree_emit<<<blocks, 256, 0, st>>>(l0, l1, level, t.nodes, t.keys, t.cnt, t.off, l1, t.gflag);
+        const cudaError_t e = cub::DeviceScan::ExclusiveSum(t.scan_temp, tb, t.cnt, t.off, bound, st);
+        if (e != cudaSuccess) return e;
         ++g_launches;
-        l0 = l1;
-        l1 += nchild;
-        ++level;
+        k_tree_next<<<1, 1, 0, st>>>(level, t.cap, t.lv, t.cnt, t.off);
+        ++g_launches;
+        k_tree_emit<<<blocks, 256, 0, st>>>(level, t.lv, t.nodes, t.keys, t.cnt, t.off, t.gflag);
+        ++g_launches;
     }
-    level_start[level + 1] = l1;
-    *nnodes = l1;
-    *depth = level;
     return cudaGetLastError();
 }
 
