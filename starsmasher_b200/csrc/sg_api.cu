@@ -527,7 +527,8 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "the tree mode takes one particle set per call");
     if (c->capturing)
         return set_err(SPHGRAV_ERR_PROTOCOL,
-                       "the tree mode cannot be captured: its build synchronises once per level");
+                       "the tree mode cannot be captured: its build reads the level table and "
+                       "the group counts back to the host");
     TRY(prepare(c, offsets, full_rows, i_lo, ni, SPHGRAV_FP64, 0));
     const Plan &P = c->plan;
     cudaStream_t st = c->stream;

@@ -159,11 +159,10 @@ struct TreeWalkArgs {
     int *err;
 };
 size_t tree_scan_temp_bytes(int n);
-// Builds the octree; returns cudaErrorMemoryAllocation (nothing else
-// changed) when `cap` nodes do not suffice.  Synchronises once per level.
-// Issues levels [level_begin, level_end) without a host wait (level 0 also
-// sets up the root); t.lv receives the level table (nodes of level l are
-// [lv[l], lv[l + 1])) and the overflow flag.
+// Octree build: issues levels [level_begin, level_end) without a host wait
+// (level 0 also sets up the root); t.lv receives the level table (nodes of
+// level l are [lv[l], lv[l + 1])) and a flag set when `cap` nodes do not
+// suffice (the caller regrows the node array and builds again).
 cudaError_t tree_build_levels(const TreeBuildArgs &t, int level_begin, int level_end,
                               cudaStream_t st);
 // Lists the walking groups (order not significant); *ngroups via `count`.
