@@ -435,13 +435,13 @@ def main():
         v64 = pairs / (ms64 * 1e-3) / 1e9
         res64 = [o.cpu().numpy() for o in outs]
         acc = accuracy(res_f32, res64)
-        peak64 = ctx.fp64_peak_probe(100000)
+        peak64 = max(ctx.fp64_peak_probe(100000) for _ in range(3))  # best of 3: clock dips
         ach64 = v64 * 1e9 * FLOPS_PER_PAIR / 1e12
         fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64, "speedup_f32split_vs_fp64": value / world / v64,
                 "roofline": {"bound": "fp64-fma", "achieved": ach64, "peak": peak64, "unit": "TFLOP/s",
                              "frac": ach64 / peak64, "flops_per_pair": FLOPS_PER_PAIR,
                              "time": "whole step (preparation included)",
-                             "peak_source": "measured in-run: DFMA throughput probe on this GPU"}}
+                             "peak_source": "measured in-run: DFMA throughput probe on this GPU, best of 3"}}
 
     # ------------------------------------- Barnes-Hut tree (approximate)
     tree = None
@@ -474,7 +474,9 @@ def main():
         ctx.set_theta(0.3)
 
     # ------------------------------------------------------------ roofline
-    peak = ctx.fp32_peak_probe(200000)
+    # best of 3 runs: a probe that lands on a clock or power dip would
+    # understate the peak and overstate the fraction
+    peak = max(ctx.fp32_peak_probe(200000) for _ in range(3))
     if kern_n == 0:
         # graph replays record no per-kernel events: time the pair kernel on
         # eager calls of the same workload instead
@@ -496,7 +498,7 @@ def main():
     roofline = {"bound": "fp32-fma", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel_ms_per_launch": kernel_ms, "flops_per_pair": FLOPS_PER_PAIR,
-                "peak_source": "measured in-run: packed-FFMA throughput probe on this GPU "
+                "peak_source": "measured in-run: packed-FFMA throughput probe on this GPU, best of 3 "
                                "(MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
                 "time_share_kernel": kernel_ms / ms_per_step if ms_per_step else None}
 
