@@ -13,11 +13,14 @@ slices equal to the full call's rows, groups handed to the direct FP64 sum
 (a point-mass core whose softening sphere holds most of the star) exact to
 1e-10, and the calls that tree mode refuses.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
 import oracle
-from conftest import err_report
+from conftest import ROOT, err_report
 from starsmasher_b200 import _lib, api, inputs
 
 pytestmark = pytest.mark.gpu
@@ -70,6 +73,20 @@ def test_error_bounded_and_growing_with_theta(gpu_ctx, star16k, direct16k):
         assert r["acc_rms"] <= b_rms and r["acc_max"] <= b_max and r["pot_rms"] <= b_pot, (theta, r)
         rms.append(r["acc_rms"])
     assert rms == sorted(rms)
+
+
+def test_more_accurate_than_reference_algorithm(gpu_ctx, star16k, direct16k):
+    """The reference's own tree algorithm, restated on the CPU
+    (oracle/tree_ref.py; its errors are the fixture
+    tests/golden/tree_ref_errors.json), against this tree mode at the
+    reference's theta = 0.3 on config 1.  The reference accepts cells inside
+    a particle's softening length as Newtonian multipoles (its softening
+    test is compiled out); this tree opens them, so every error is lower."""
+    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "tree_ref_errors.json")))
+    ref = ref["config1"]["theta_0.3"]
+    r = err_report(*_tree(gpu_ctx, star16k, 0.3), *direct16k[0])
+    for k in ("acc_rms", "acc_max", "pot_rms", "pot_max"):
+        assert r[k] <= ref[k], (k, r[k], ref[k])
 
 
 def test_deterministic_and_row_slice(gpu_ctx, star16k):
