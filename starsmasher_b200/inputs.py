@@ -144,6 +144,18 @@ def _pack(parts: List[tuple], name: str, meta: dict) -> ParticleSets:
                         np.array(offs, dtype=np.int32), name, meta)
 
 
+def from_snapshots(paths: List[str]) -> ParticleSets:
+    """Real models as a batch: one set per dump file (sph.start*u, out*.sph),
+    with range2 built as the gravity call builds it (grav.f:15-18)."""
+    from .snapshot import read_snapshot
+    parts = []
+    for path in paths:
+        s = read_snapshot(path)
+        pos = np.stack([s.data["x"], s.data["y"], s.data["z"]], axis=1)
+        parts.append((pos, s.data["am"].copy(), s.range2()))
+    return _pack(parts, "snapshots", {"paths": list(paths)})
+
+
 def single_polytrope(n: int, n_index: float = 1.5, seed: int = 1, mass: float = 1.0,
                      radius: float = 1.0) -> ParticleSets:
     rng = np.random.default_rng(seed)

@@ -111,3 +111,24 @@ def test_snapshot_writer_reproduces_reference_dumps(tmp_path, case):
     write_snapshot(out, read_snapshot(src))
     with open(src, "rb") as a, open(out, "rb") as b:
         assert a.read() == b.read()
+
+
+def test_snapshots_as_a_batch(tmp_path):
+    """Dump files become one particle set each, range2 = +-4 hp^2 (grav.f:15-18)."""
+    from starsmasher_b200.snapshot import FIELDS
+    rng = np.random.default_rng(3)
+    paths = []
+    for k, n in enumerate((40, 75)):
+        data = {f: rng.uniform(0.1, 1.0, n) for f in FIELDS}
+        data["u"][::7] = 0.0  # point masses
+        p = str(tmp_path / f"m{k}.sph")
+        write_snapshot(p, Snapshot(n, data))
+        paths.append((p, data))
+    b = inputs.from_snapshots([p for p, _ in paths])
+    assert b.nsets == 2 and list(b.offsets) == [0, 40, 115]
+    for s, (_, d) in enumerate(paths):
+        a, e = b.offsets[s], b.offsets[s + 1]
+        np.testing.assert_array_equal(b.x[a:e], d["x"])
+        np.testing.assert_array_equal(b.m[a:e], d["am"])
+        want = np.where(d["u"] == 0.0, -4.0 * d["hp"] ** 2, 4.0 * d["hp"] ** 2)
+        np.testing.assert_array_equal(b.range2[a:e], want)
