@@ -168,16 +168,23 @@ def body_node(p: np.ndarray, M: np.ndarray, com: np.ndarray, q: np.ndarray):
     return acc, pot
 
 
-def forces(x, y, z, m, range2, theta: float, nkernel: int = 0):
-    """The reference tree's (ax, ay, az, pot) for every particle, in input order."""
+def forces(x, y, z, m, range2, theta: float, nkernel: int = 0, only=None):
+    """The reference tree's (ax, ay, az, pot) for every particle, in input
+    order.  With ``only`` (input indices), just the groups holding those
+    particles are walked; the other rows come back as NaN."""
     pos = np.stack([x, y, z], axis=1).astype(np.float64)
     n = pos.shape[0]
     keys = hilbert_keys(pos)
     order = np.argsort(keys, kind='stable')
     ps, ms, r2s = pos[order], np.asarray(m, np.float64)[order], np.asarray(range2, np.float64)[order]
     tree = Tree(ps, ms, keys[order], theta)
-    out = np.zeros((n, 4))
-    for g0 in range(0, n, NCRIT):
+    out = np.full((n, 4), np.nan)
+    starts = range(0, n, NCRIT)
+    if only is not None:
+        inv = np.empty(n, dtype=np.int64)
+        inv[order] = np.arange(n)
+        starts = sorted(set(int(g) for g in (inv[np.asarray(only)] // NCRIT) * NCRIT))
+    for g0 in starts:
         g1 = min(g0 + NCRIT, n)
         gp = ps[g0:g1]
         lo, hi = gp.min(axis=0), gp.max(axis=0)
@@ -198,6 +205,6 @@ def forces(x, y, z, m, range2, theta: float, nkernel: int = 0):
         pot += pp
         out[g0:g1, :3] = acc
         out[g0:g1, 3] = pot
-    res = np.zeros((n, 4))
+    res = np.empty((n, 4))
     res[order] = out
     return res[:, 0], res[:, 1], res[:, 2], res[:, 3]
