@@ -37,3 +37,16 @@ def test_config1_errors_match_fixture():
     r = err_report(*tree_ref.forces(s.x, s.y, s.z, s.m, s.range2, 0.3), *want)
     for k in ("acc_rms", "acc_max", "pot_rms", "pot_max"):
         assert abs(r[k] - ref["theta_0.3"][k]) <= 1e-3 * ref["theta_0.3"][k], (k, r[k], ref["theta_0.3"][k])
+
+
+def test_sampled_groups_equal_the_full_walk():
+    """Walking only the groups that hold chosen particles (how config 3 is
+    sampled) gives exactly the full walk's rows and NaN elsewhere."""
+    s = inputs.single_polytrope(3000, 1.5, seed=3)
+    full = tree_ref.forces(s.x, s.y, s.z, s.m, s.range2, 0.3)
+    part = tree_ref.forces(s.x, s.y, s.z, s.m, s.range2, 0.3, only=np.array([0, 5, 1000, 2999]))
+    rows = np.flatnonzero(~np.isnan(part[0]))
+    assert 4 <= rows.size <= 4 * tree_ref.NCRIT
+    assert {0, 5, 1000, 2999} <= set(rows.tolist())
+    for a, b in zip(part, full):
+        np.testing.assert_array_equal(a[rows], b[rows])
