@@ -9,14 +9,21 @@ cpu_grav.f) on a bounded sample reported beside it.
 One step = one gravity call over the whole workload with inputs resident in
 HBM (``value``); ``e2e`` repeats it through the reference-facing Fortran
 C-ABI (firsthalf_grav_forces_/lasthalf_grav_forces_) from host arrays, copies
-included.  Default workload: config3, the N=1,048,576 red-giant model.
+included.  Default workload: config3, the N=1,048,576 red-giant model; the
+default run also measures the batched launch on config4 (64 uneven models,
+against one call per model) and the graph-captured sweep on config5
+(``config4_batched``, ``config5_graph_sweep``).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--workload config1..config5]
 
-Multi-GPU (torchrun): every rank evaluates its own independent copy of the
-workload (a different seed: independent stellar models, no data-path
-collective), ``value`` = all ranks' pairs / the slowest rank's time.
+Multi-GPU (torchrun, one process per GPU): the reference's own split of the
+gravity rows across GPU ranks (main.f:283-295).  Every rank holds its own
+rows' positions; each step all-gathers the five source arrays over NCCL,
+evaluates the rank's rows against all n sources and all-gathers the results
+(balAV3.f:423-434 gathers them too).  The total work is fixed as N grows
+(strong scaling); ``value`` = all pairs / the slowest rank's time.  Batched
+workloads are sharded by whole sets instead.
 """
 from __future__ import annotations
 
@@ -53,10 +60,18 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the config4 (batched) and config5 (graph sweep) sections")
+    p.add_argument("--graph-calls", type=int, default=20,
+                   help="timed graph replays in the config5 section (and with --graph)")
     p.add_argument("--variant", type=int, default=-1,
                    help="force a kernel variant of --precision (default: tuned/automatic)")
-    p.add_argument("--fp64-band", type=float, default=2.0,
-                   help="split-FP32: pairs with r < band * max(H) are evaluated in FP64")
+    p.add_argument("--fp64-band", type=float, default=None,
+                   help="split-FP32: pairs with r < band * max(H) are evaluated in FP64 "
+                        "(default: the library's)")
+    p.add_argument("--refine", type=float, default=None,
+                   help="split-FP32: FP64 refine of rows with error scale G > T |a| "
+                        "(default: the library's; 0 = off)")
     p.add_argument("--graph", action="store_true",
                    help="batched workloads: each step replays a captured CUDA graph of "
                         "(seeded 1e-3 position kick + gravity) on device-resident state")
@@ -128,7 +143,7 @@ def dist_setup(args):
     return world, rank, local
 
 
-def cpu_baseline(ws, target_s: float, rank_seed_rows: int = 0):
+def cpu_baseline(ws, target_s: float):
     """The reference's CPU path (oracle: C restatement of cpu_grav.f, the
     j >= i triangle with Newton's third law, all host cores) on a bounded
     sample of rows of the same workload; credited ordered pairs = 2 x triangle
@@ -178,14 +193,14 @@ def cpu_baseline(ws, target_s: float, rank_seed_rows: int = 0):
     return {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
 
 
-def load_workload(name: str, rank: int):
+def load_workload(name: str):
     """configN (the five benchmark workloads) or polytrope:N (one equal-mass
     n=3 polytrope of N particles, for small profiling cases)."""
     from starsmasher_b200 import inputs
     if name.startswith("polytrope:"):
         n = int(name.split(":")[1])
-        return inputs.single_polytrope(n, 3.0, seed=10 + 100 * rank)
-    seed = {"config1": 1, "config2": 2, "config3": 3, "config4": 4, "config5": 5}[name] + 100 * rank
+        return inputs.single_polytrope(n, 3.0, seed=10)
+    seed = {"config1": 1, "config2": 2, "config3": 3, "config4": 4, "config5": 5}[name]
     return inputs.cached(name, seed=seed)
 
 
@@ -214,7 +229,7 @@ def run_reference_arm(args, world, rank):
     oracle/ is timed) on all host cores, K bounded samples of the workload."""
     if rank != 0:
         return
-    ws = load_workload(args.workload, 0)
+    ws = load_workload(args.workload)
     for _ in range(args.warmup):
         cpu_baseline(ws, 0.5)
     vals = []
@@ -230,13 +245,128 @@ def run_reference_arm(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": ws.name, "n": ws.n, "nsets": ws.nsets, "pairs_per_step": ws.pairs,
                    "nkernel": 0, "algorithm": "cpu_grav.f triangle (C restatement), sampled rows"},
         "cpu_baseline": dict(last, value=value),
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+class Timer:
+    """CUDA-event timing of steps on one stream, with an L2 flush (a 256 MB
+    write, > 126 MB of L2) before every timed step."""
+
+    def __init__(self, torch, stream, device):
+        self.torch = torch
+        self.stream = stream
+        self.flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")
+
+    def run(self, fn, steps):
+        torch = self.torch
+        evs = []
+        for _ in range(steps):
+            self.flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            fn()
+            e1.record(self.stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / max(1, steps)
+
+
+def upload(torch, ws, device):
+    dt = torch.float64
+    X = [torch.as_tensor(a).to(device=f"cuda:{device}", dtype=dt)
+         for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
+    outs = [torch.empty(ws.n, dtype=dt, device=f"cuda:{device}") for _ in range(4)]
+    return X, outs
+
+
+def config4_section(torch, ctx, timer, device, args):
+    """The batched persistent launch on the uneven-N batch (config4): one
+    batched call against one call per model (split-FP32, and plain FP64),
+    with its accuracy against the FP64 kernel."""
+    ws = load_workload("config4")
+    X, outs = upload(torch, ws, device)
+
+    def batched(prec="f32split"):
+        ctx.batch_forces_device(ws.offsets, *X, *outs, nkernel=args.nkernel, precision=prec)
+
+    def separate(prec="f32split"):
+        for s in range(ws.nsets):
+            a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
+            ctx.forces_device(b - a, *(t[a:b] for t in X), *(o[a:b] for o in outs),
+                              nkernel=args.nkernel, precision=prec)
+
+    batched()
+    torch.cuda.synchronize()
+    ms_b = timer.run(batched, 3)
+    res32 = [o.cpu().numpy() for o in outs]
+    refined = ctx.last_refine_rows()
+    separate()
+    torch.cuda.synchronize()
+    ms_s = timer.run(separate, 2)
+    separate("fp64")
+    ms_s64 = timer.run(lambda: separate("fp64"), 1)
+    batched("fp64")
+    ms_b64 = timer.run(lambda: batched("fp64"), 1)
+    res64 = [o.cpu().numpy() for o in outs]
+    pairs = ws.pairs
+    return {"workload": ws.name, "n": ws.n, "nsets": ws.nsets, "pairs_per_step": pairs,
+            "batched_ms": ms_b, "batched_value": pairs / (ms_b * 1e-3) / 1e9,
+            "separate_calls_ms": ms_s, "speedup_batched_vs_separate": ms_s / ms_b,
+            "separate": f"{ws.nsets} sphgrav_forces_device calls, one per model (split-FP32)",
+            "separate_fp64_calls_ms": ms_s64, "speedup_batched_vs_separate_fp64": ms_s64 / ms_b,
+            "batched_fp64_ms": ms_b64, "speedup_f32split_vs_fp64_batched": ms_b64 / ms_b,
+            "refined_rows": refined, "accuracy_vs_fp64": accuracy(res32, res64),
+            "l2": "flushed before every timed call"}
+
+
+def config5_section(torch, ctx, timer, stream, device, args):
+    """The graph-captured sweep (config5): a CUDA graph of (seeded position
+    kick, sigma = 1e-3 R, + batched gravity) replayed on device-resident
+    state; time per replay and the accuracy at call 1 and at the last call
+    against the FP64 kernel on the same kicked positions."""
+    from starsmasher_b200 import Context
+    ws = load_workload("config5")
+    X, outs = upload(torch, ws, device)
+    sigma, seed = 1e-3, 12345
+    o64 = [torch.empty_like(o) for o in outs]
+
+    def fp64_now():
+        ctx.batch_forces_device(ws.offsets, *X, *o64, nkernel=args.nkernel, precision="fp64")
+        torch.cuda.synchronize()
+        return [o.cpu().numpy() for o in o64]
+
+    with Context(device) as g:
+        g.set_stream(stream.cuda_stream)
+        g.batch_forces_device(ws.offsets, *X, *outs, nkernel=args.nkernel, precision="f32split")
+        torch.cuda.synchronize()
+        g.kick_reset(0)
+        with g.capture() as cap:
+            g.kick_device(ws.n, X[0], X[1], X[2], sigma, seed)
+            g.batch_forces_device(ws.offsets, *X, *outs, nkernel=args.nkernel, precision="f32split")
+        graph = cap.graph
+        graph.launch(1)
+        torch.cuda.synchronize()
+        first = [o.cpu().numpy() for o in outs]
+        acc1 = accuracy(first, fp64_now())
+        ms = timer.run(lambda: graph.launch(1), args.graph_calls)
+        calls = 1 + args.graph_calls
+        last = [o.cpu().numpy() for o in outs]
+        refined = g.last_refine_rows()
+        graph.close()
+    acc_last = accuracy(last, fp64_now())
+    return {"workload": ws.name, "n": ws.n, "nsets": ws.nsets, "pairs_per_call": ws.pairs,
+            "ms_per_call": ms, "value": ws.pairs / (ms * 1e-3) / 1e9, "calls_timed": args.graph_calls,
+            "calls_total": calls, "kick_sigma": sigma,
+            "graph": "kick + keys/sort/gather/tiles + pair kernel + merge + FP64 refine, one CUDA graph",
+            "refined_rows_last_call": refined, "accuracy_call_1": acc1,
+            f"accuracy_call_{calls}": acc_last, "l2": "flushed before every timed replay"}
 
 
 def main():
@@ -250,7 +380,7 @@ def main():
     import torch.distributed as dist
     from datetime import timedelta
 
-    from starsmasher_b200 import Context, api, launch_count
+    from starsmasher_b200 import Context, api, launch_count, multirank
 
     if world > 1:
         torch.cuda.set_device(local)
@@ -259,25 +389,27 @@ def main():
     device = local if world > 1 else 0
     torch.cuda.set_device(device)
 
-    ws = load_workload(args.workload, rank)
+    # every rank loads the same model; the ranks divide its work
+    ws = load_workload(args.workload)
     n = ws.n
     pairs = ws.pairs
     batched = ws.nsets > 1
 
-    # one dedicated stream for the library, the L2 flush and the timing events
+    # one dedicated stream for the library, the collectives, the flush and the events
     stream = torch.cuda.Stream(device=device)
     torch.cuda.set_stream(stream)
     ctx = Context(device)
     ctx.set_stream(stream.cuda_stream)
     if args.variant >= 0:
         ctx.force_variant(args.precision, args.variant)
-    ctx.set_fp64_band(args.fp64_band)
+    if args.fp64_band is not None:
+        ctx.set_fp64_band(args.fp64_band)
+    if args.refine is not None:
+        ctx.set_refine(args.refine)
+    timer = Timer(torch, stream, device)
 
-    dt = torch.float64
-    X = [torch.as_tensor(a).to(device=f"cuda:{device}", dtype=dt)
-         for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
-    outs = [torch.empty(n, dtype=dt, device=f"cuda:{device}") for _ in range(4)]
-    W = torch.empty(ws.nsets, dtype=dt, device=f"cuda:{device}")
+    X, outs = upload(torch, ws, device)
+    W = torch.empty(ws.nsets, dtype=torch.float64, device=f"cuda:{device}")
 
     def gravity(precision):
         if batched:
@@ -286,26 +418,51 @@ def main():
         else:
             ctx.forces_device(n, *X, *outs, W=W, nkernel=args.nkernel, precision=precision)
 
+    # ----------------------------------------------------- the step
+    if world == 1:
+        mode = "single GPU"
+
+        def step(precision):
+            gravity(precision)
+    elif not batched:
+        # the reference's gravity row split: this rank owns rows [lo, hi)
+        lo, hi = multirank.gpu_row_range(n, world, rank)
+        own = torch.stack([t[lo:hi] for t in X]).contiguous()
+        compute = {p: multirank.gpu_compute_device(ctx, args.nkernel, p) for p in ("f32split", "fp64")}
+        mode = f"row split x{world} (main.f:283-295): NCCL all-gather of sources and rows"
+        split_out = {}
+
+        def step(precision):
+            src, res = multirank.forces_row_split_device(compute[precision], own, n)
+            split_out["res"] = res
+    else:
+        shards = multirank.shard_sets(np.diff(ws.offsets), world)[rank]
+        sub = [(int(ws.offsets[s]), int(ws.offsets[s + 1])) for s in shards]
+        offs = np.concatenate([[0], np.cumsum([b - a for a, b in sub])]).astype(np.int32)
+        Xs = [torch.cat([t[a:b] for a, b in sub]) if sub else t[:0] for t in X]
+        outs_s = [torch.empty_like(t) for t in Xs[:4]]
+        mode = f"set shard x{world}: whole models per rank, longest first"
+
+        def step(precision):
+            if sub:
+                ctx.batch_forces_device(offs, *Xs, *outs_s, nkernel=args.nkernel,
+                                        precision=precision)
+
     graph = None
     sigma, kick_seed = 1e-3, 12345
 
-    def step(precision):
+    def timed_step(precision):
         if graph is not None and precision == args.precision:
             graph.launch(1)
         else:
-            gravity(precision)
-
-    # L2 flush buffer (> 126 MB L2), written between timed steps
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")
+            step(precision)
 
     for _ in range(max(3, args.warmup)):
-        gravity(args.precision)
+        step(args.precision)
     torch.cuda.synchronize()
     acc_first_call = None
     calls = 0
-    if args.graph:
-        # device-resident sweep: every replay kicks the positions (seeded,
-        # sigma = 1e-3 R) and recomputes gravity, all inside one CUDA graph
+    if args.graph and world == 1:
         ctx.kick_reset(0)
         with ctx.capture() as cap:
             ctx.kick_device(n, X[0], X[1], X[2], sigma, kick_seed)
@@ -314,8 +471,6 @@ def main():
         graph.launch(1)
         calls = 1
         if not args.no_fp64:
-            # error of call 1 against the FP64 kernel on the same kicked
-            # positions, on a second context so that the graph's plan stays
             with Context(device) as ctx64:
                 ctx64.set_stream(stream.cuda_stream)
                 o64 = [torch.empty_like(o) for o in outs]
@@ -344,34 +499,24 @@ def main():
     torch.cuda.synchronize()
     clocks.start()
     l0 = launch_count()
-    evs = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step(args.precision)
-        e1.record(stream)
-        evs.append((e0, e1))
-    torch.cuda.synchronize()
+    ms_per_step = timer.run(lambda: timed_step(args.precision), args.steps)
     barrier()
     launches = launch_count() - l0
     clk = clocks.stop()
     kern_ms, kern_n = ctx.profile_read()
     ctx.profile_enable(False)
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{device}")
+        t = torch.tensor([ms_per_step], dtype=torch.float64, device=f"cuda:{device}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    value = pairs * world * args.steps / (total_ms * 1e-3) / 1e9
-    res_f32 = [o.cpu().numpy() for o in outs]
+        ms_per_step = float(t.item())
+    value = pairs / (ms_per_step * 1e-3) / 1e9
+    refined = ctx.last_refine_rows() if world == 1 else None
+    res_f32 = [o.cpu().numpy() for o in outs] if world == 1 else None
     graph_info = None
     if graph is not None:
         calls += args.steps
         graph_info = {"calls_timed": args.steps, "ms_per_call": ms_per_step,
-                      "kick_sigma": sigma, "nodes": "kick + sort/gather/tiles + pair kernel + merge",
+                      "kick_sigma": sigma, "nodes": "kick + keys/sort/gather/tiles + pair kernel + merge + refine",
                       "calls_total": calls, "accuracy_call_1": acc_first_call,
                       "accuracy_last_call": f"accuracy_vs_fp64 (call {calls})"}
         graph.close()
@@ -379,37 +524,17 @@ def main():
 
     # ------------------------------------- batched vs one call per set
     batch_cmp = None
-    if batched and not args.no_separate:
-        def separate():
+    if world == 1 and batched and not args.no_separate:
+        def separate(prec):
             for s in range(ws.nsets):
                 a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
                 ctx.forces_device(b - a, *(t[a:b] for t in X), *(o[a:b] for o in outs),
-                                  nkernel=args.nkernel, precision=args.precision)
-        separate()
+                                  nkernel=args.nkernel, precision=prec)
+        separate(args.precision)
         torch.cuda.synchronize()
-        reps = max(1, min(args.steps, 3))
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            separate()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        sep_ms = e0.elapsed_time(e1) / reps
-        # the same with the plain FP64 kernel: the other reading of "separate
-        # plain launches"
-        def separate_fp64():
-            for s_ in range(ws.nsets):
-                a, b = int(ws.offsets[s_]), int(ws.offsets[s_ + 1])
-                ctx.forces_device(b - a, *(t[a:b] for t in X), *(o[a:b] for o in outs),
-                                  nkernel=args.nkernel, precision="fp64")
-        separate_fp64()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        separate_fp64()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        sep64_ms = e0.elapsed_time(e1)
+        sep_ms = timer.run(lambda: separate(args.precision), max(1, min(args.steps, 3)))
+        separate("fp64")
+        sep64_ms = timer.run(lambda: separate("fp64"), 1)
         batch_cmp = {"separate_calls_ms_per_step": sep_ms, "batched_ms_per_step": ms_per_step,
                      "speedup_batched_vs_separate": sep_ms / ms_per_step,
                      "separate": f"{ws.nsets} sphgrav_forces_device calls, one per set",
@@ -420,24 +545,17 @@ def main():
     fp64 = None
     acc = None
     res64 = None
-    if not args.no_fp64:
+    if world == 1 and not args.no_fp64:
         step("fp64")
         torch.cuda.synchronize()
-        reps = 2
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            step("fp64")
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms64 = e0.elapsed_time(e1) / reps
+        ms64 = timer.run(lambda: step("fp64"), 2)
         v64 = pairs / (ms64 * 1e-3) / 1e9
         res64 = [o.cpu().numpy() for o in outs]
         acc = accuracy(res_f32, res64)
         peak64 = max(ctx.fp64_peak_probe(100000) for _ in range(3))  # best of 3: clock dips
         ach64 = v64 * 1e9 * FLOPS_PER_PAIR / 1e12
-        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64, "speedup_f32split_vs_fp64": value / world / v64,
+        fp64 = {"value": v64, "unit": UNIT, "ms_per_step": ms64,
+                "speedup_f32split_vs_fp64": value / v64,
                 "roofline": {"bound": "fp64-fma", "achieved": ach64, "peak": peak64, "unit": "TFLOP/s",
                              "frac": ach64 / peak64, "flops_per_pair": FLOPS_PER_PAIR,
                              "time": "whole step (preparation included)",
@@ -446,10 +564,10 @@ def main():
     # ------------------------------------- Barnes-Hut tree (approximate)
     tree = None
     thetas = [float(v) for v in args.tree_thetas.split(",") if v.strip()]
-    if not batched and thetas and res64 is not None:
+    if world == 1 and not batched and thetas and res64 is not None:
         tree = {"what": "SPHGRAV_TREE: octree, quadrupole nodes, FP64 softened pairs; "
                         "approximate, error set by theta (not the direct-sum metric)",
-                "time": "whole call, device arrays (build syncs once per tree level)",
+                "time": "whole call, device arrays (build syncs once per 4 tree levels)",
                 "direct_f32split_ms_per_step": ms_per_step}
         for th in thetas:
             ctx.set_theta(th)
@@ -457,15 +575,7 @@ def main():
             torch.cuda.synchronize()
             res_t = [o.cpu().numpy() for o in outs]
             ngroups, nheavy = ctx.tree_stats()
-            reps = 3
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(reps):
-                gravity("tree")
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms_t = e0.elapsed_time(e1) / reps
+            ms_t = timer.run(lambda: gravity("tree"), 3)
             tree[f"theta_{th:g}"] = {
                 "ms_per_step": ms_t, "speedup_vs_f32split_direct": ms_per_step / ms_t,
                 "speedup_vs_fp64_direct": fp64["ms_per_step"] / ms_t,
@@ -483,11 +593,12 @@ def main():
         ctx.profile_enable(True)
         ctx.profile_read()
         for _ in range(2):
-            gravity(args.precision)
+            step(args.precision)
         kern_ms, kern_n = ctx.profile_read()
         ctx.profile_enable(False)
     kernel_ms = kern_ms / max(1, kern_n)
-    achieved = pairs * FLOPS_PER_PAIR / (kernel_ms * 1e-3) / 1e12
+    kernel_pairs = pairs if world == 1 else pairs / world
+    achieved = kernel_pairs * FLOPS_PER_PAIR / (kernel_ms * 1e-3) / 1e12
     # DRAM bytes of one pair-kernel launch on this workload, from a one-pass
     # ncu capture of this same command (profiles/traffic_*.json), if recorded
     traffic = None
@@ -505,11 +616,26 @@ def main():
     # ----------------------------------------------------------------- e2e
     e2e = None
     if not args.no_e2e:
-        if batched:
+        if world > 1 and not batched:
+            # host arrays: this rank's rows in pinned memory, copied in every
+            # step; the gathered result read back every step
+            own_h = torch.stack([torch.as_tensor(a[lo:hi]) for a in
+                                 (ws.x, ws.y, ws.z, ws.m, ws.range2)]).pin_memory()
+            res_h = torch.empty((4, n), dtype=torch.float64).pin_memory()
+
+            def e2e_step():
+                own_d = own_h.to(f"cuda:{device}", non_blocking=True)
+                src, res = multirank.forces_row_split_device(compute[args.precision], own_d, n)
+                res_h.copy_(res, non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+            how = "row split from host arrays (pinned H2D of own rows, D2H of all rows)"
+            h2d, d2h = 5 * 8 * (hi - lo), 4 * 8 * n
+        elif batched:
             def e2e_step():
                 ctx.batch_forces(ws.offsets, ws.x, ws.y, ws.z, ws.m, ws.range2, args.nkernel,
                                  args.precision)
             how = "sphgrav_batch_forces (host arrays)"
+            h2d, d2h = 5 * 8 * n, 4 * 8 * n
         else:
             api.gpu_init_dev(device, 0.3)
             api.set_legacy_precision(args.precision)
@@ -520,38 +646,48 @@ def main():
                                           args.nkernel)
                 api.lasthalf_grav_forces(n, gx, gy, gz, gp)
             how = "firsthalf_grav_forces_/lasthalf_grav_forces_ (Fortran C-ABI, host arrays)"
-        e2e_step()
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
+            h2d, d2h = 5 * 8 * n, 4 * 8 * n
+        if world == 1 or not batched:
             e2e_step()
-        t_e2e = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{device}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t.item())
-        e2e = {"value": pairs * world * args.steps / t_e2e / 1e9, "unit": UNIT,
-               "h2d_bytes_per_step": 5 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n,
-               "ms_per_step": t_e2e / args.steps * 1e3, "path": how}
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                e2e_step()
+            t_e2e = time.perf_counter() - t0
+            if world > 1:
+                t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{device}")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                t_e2e = float(t.item())
+            e2e = {"value": pairs * args.steps / t_e2e / 1e9, "unit": UNIT,
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "ms_per_step": t_e2e / args.steps * 1e3, "path": how}
+
+    # -------------------------------- config4 / config5 sections (1 GPU)
+    extras = {}
+    if world == 1 and args.workload == "config3" and not args.no_extras:
+        extras["config4_batched"] = config4_section(torch, ctx, timer, device, args)
+        extras["config5_graph_sweep"] = config5_section(torch, ctx, timer, stream, device, args)
 
     # -------------------------------------------------------- CPU baseline
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(ws, args.cpu_seconds)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "f32split" else "f64",
-            "data": "synthetic: seeded polytropic star models (no public dataset), one independent model per rank",
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "f32split" else "f64",
+            "data": "synthetic: seeded polytropic star models (no public dataset)",
             "config": {"workload": ws.name, "n": n, "nsets": ws.nsets, "pairs_per_step": pairs,
                        "precision": args.precision, "nkernel": args.nkernel,
-                       "fp64_band": args.fp64_band,
-                       "l2": "flushed between timed steps (256 MB write)",
-                       "parallelism": f"replicas x{world} (independent models per GPU)"},
+                       "fp64_band": args.fp64_band if args.fp64_band is not None else "library default",
+                       "refine": args.refine if args.refine is not None else "library default",
+                       "l2": "flushed before every timed step (256 MB write)",
+                       "parallelism": mode},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "fp64": fp64, "accuracy_vs_fp64": acc,
+            "clocks": clk, "fp64": fp64, "accuracy_vs_fp64": acc, "refined_rows": refined,
         }
         if batch_cmp:
             line["batch_vs_separate"] = batch_cmp
@@ -559,6 +695,7 @@ def main():
             line["graph_sweep"] = graph_info
         if tree:
             line["tree"] = tree
+        line.update(extras)
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -19,10 +19,11 @@
  *                      rsqrt.approx (variants named *_newton add one Newton
  *                      step) summed into compensated (Kahan/TwoSum) partial
  *                      sums; FP64 for the split, the cross-block partial sums,
- *                      the pairs with r < band * max H (band 2 by default,
- *                      sphgrav_set_fp64_band) and the potential-energy
- *                      diagnostic.  Max relative error of the acceleration is
- *                      ~1e-6 or better for well-conditioned particles.
+ *                      the pairs with r < band * max H (band 1 by default,
+ *                      sphgrav_set_fp64_band), the rows whose FP32 sums are
+ *                      ill-conditioned (sphgrav_set_refine) and the
+ *                      potential-energy diagnostic.  Max relative error of the
+ *                      acceleration below 1e-6 on the benchmark workloads.
  *   SPHGRAV_TREE       Barnes-Hut octree, the approximate alternative the
  *                      reference ships with the same ABI
  *                      (misc/SPHgravtree_lib): monopole + quadrupole cells,
@@ -211,11 +212,33 @@ int sphgrav_autotune(sphgrav_ctx *ctx, int nsets, const int *offsets,
 int sphgrav_tuning_save(sphgrav_ctx *ctx, const char *path);
 int sphgrav_tuning_load(sphgrav_ctx *ctx, const char *path);
 /* Split-FP32 only: pairs with r < factor * max(H_i, H_j) are evaluated in
- * FP64 (default 2.0; 1.0 = only the softened near field, r < max H).  A wider
+ * FP64 (default 1.0 = only the softened near field, r < max H).  A wider
  * band lowers the error of particles whose acceleration cancels and costs
  * time in proportion to the pairs it moves (~factor^3 times the near-field
  * pairs).  Factor in [1, 16].  No reference counterpart. */
 int sphgrav_set_fp64_band(sphgrav_ctx *ctx, double factor);
+/* Split-FP32 only: FP64 refine of ill-conditioned rows.  The split-FP32
+ * kernel keeps, per row, G = sqrt(sum over its 256-source j-tiles of
+ * |FP32 tile sum of the acceleration|^2), the scale of its FP32 rounding
+ * error.  Rows with G > threshold * |a| -- particles whose acceleration
+ * cancels, e.g. near a star's centre or between two stars -- are recomputed
+ * in FP64 on the device in the same call (no host round trip; capturable),
+ * so their relative error is that of the FP64 kernel.  Rows lying more than
+ * 8 H from the centre of their row tile (where the FP32 rounding of their
+ * tile-relative position shifts them measurably) are recomputed too.
+ * Default 1.0 (0.1-0.4% of the rows of the benchmark workloads); 0 turns the
+ * refine off.  No reference counterpart. */
+int sphgrav_set_refine(sphgrav_ctx *ctx, double threshold);
+/* Rows the last split-FP32 call recomputed in FP64 (0 when the refine was
+ * off or the call was not split-FP32).  Synchronises the context's stream. */
+int sphgrav_last_refine_rows(sphgrav_ctx *ctx, long long *rows);
+/* Keep (on != 0) the per-row error scale G of later split-FP32 calls, and
+ * copy the last call's G (caller order, n = all particles of the call) to
+ * host memory; rows far from their tile centre read +infinity.
+ * sphgrav_error_scale returns SPHGRAV_ERR_PROTOCOL when the last call kept
+ * no scale of n rows.  Diagnostics; no reference counterpart. */
+int sphgrav_keep_error_scale(sphgrav_ctx *ctx, int on);
+int sphgrav_error_scale(sphgrav_ctx *ctx, int n, double *G);
 /* SPHGRAV_TREE: opening angle theta in [0, 2] (default 0.3, the value
  * main.f:269 passes to gpu_init_dev_).  A node is opened when the gap
  * between its box and the walking group's box is at most l / theta (l its

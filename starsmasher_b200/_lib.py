@@ -60,6 +60,10 @@ SIGNATURES = {
     "sphgrav_tuning_load": (_I, [_P, ctypes.c_char_p]),
     "sphgrav_force_variant": (_I, [_P, _I, _I]),
     "sphgrav_set_fp64_band": (_I, [_P, _D]),
+    "sphgrav_set_refine": (_I, [_P, _D]),
+    "sphgrav_last_refine_rows": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    "sphgrav_keep_error_scale": (_I, [_P, _I]),
+    "sphgrav_error_scale": (_I, [_P, _I, _P]),
     "sphgrav_set_theta": (_I, [_P, _D]),
     "sphgrav_tree_stats": (_I, [_P, _PI, _PI]),
     "sphgrav_variant_count": (_I, [_I]),

@@ -133,8 +133,29 @@ class Context:
         return g.value, h.value
 
     def set_fp64_band(self, factor: float) -> None:
-        """Split-FP32: evaluate pairs with r < factor * max(H) in FP64 (default 2)."""
+        """Split-FP32: evaluate pairs with r < factor * max(H) in FP64 (default 1)."""
         check(self._lib.sphgrav_set_fp64_band(self._h, float(factor)), "sphgrav_set_fp64_band")
+
+    def set_refine(self, threshold: float) -> None:
+        """Split-FP32: recompute in FP64 the rows whose error scale G exceeds
+        threshold * |a| (default 1.0; 0 turns the refine off)."""
+        check(self._lib.sphgrav_set_refine(self._h, float(threshold)), "sphgrav_set_refine")
+
+    def last_refine_rows(self) -> int:
+        """Rows the last split-FP32 call recomputed in FP64 (synchronises)."""
+        v = ctypes.c_longlong(0)
+        check(self._lib.sphgrav_last_refine_rows(self._h, ctypes.byref(v)), "sphgrav_last_refine_rows")
+        return int(v.value)
+
+    def keep_error_scale(self, on: bool = True) -> None:
+        """Keep the per-row error scale G of later split-FP32 calls."""
+        check(self._lib.sphgrav_keep_error_scale(self._h, 1 if on else 0), "sphgrav_keep_error_scale")
+
+    def error_scale(self, n: int) -> np.ndarray:
+        """G of the last split-FP32 call (caller order, all n particles)."""
+        out = np.zeros(n)
+        check(self._lib.sphgrav_error_scale(self._h, int(n), _hp(out)), "sphgrav_error_scale")
+        return out
 
     def plan_info(self) -> dict:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -151,6 +151,11 @@ struct sphgrav_graph {
     unsigned long long epoch = 0;
 };
 
+// Default refine threshold T of split-FP32 calls: rows whose error scale G
+// (the root sum of squares of their FP32 tile sums) exceeds T |a| are
+// recomputed in FP64.
+static const double kRefineDefault = 1.0;
+
 struct sphgrav_ctx {
     int device = 0;
     int sm_count = 148;
@@ -178,6 +183,17 @@ struct sphgrav_ctx {
     DBuf<double> partials, wtile, wdev;
     DBuf<unsigned long long> kick_counter;
     DBuf<double> range2;  // sphgrav_gravforce_device: range2 built on the device
+
+    // FP64 refine of split-FP32 rows whose error scale G exceeds refine_T |a|
+    double refine_T = kRefineDefault;  // 0: off
+    bool keep_scale = false;           // keep G per row (sphgrav_error_scale)
+    int scale_n = 0;                   // rows of the kept G (0: none)
+    int refine_nsets = 0;              // sets of the last split-FP32 call (rcount entries)
+    DBuf<float> gpart;                 // [slot][itile] G^2 partials
+    DBuf<int> rcount, rlist, rnitems, rhead;
+    DBuf<SetDesc> rsets;
+    DBuf<WorkItem> ritems;
+    DBuf<double> rpart, scale;
 
     // Barnes-Hut mode (SPHGRAV_TREE)
     double theta = 0.3;   // opening angle (gpu_init_dev_ passes it; main.f:269)
@@ -208,7 +224,7 @@ struct sphgrav_ctx {
     std::map<int, std::string> tuned[2];  // N bucket -> variant name
 
     // kernel timing (sphgrav_profile_*)
-    double fp64_band = 2.0;  // split-FP32: FP64 for r < fp64_band * max(H)
+    double fp64_band = 1.0;  // split-FP32: FP64 for r < fp64_band * max(H)
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
@@ -254,6 +270,9 @@ static int use_device(sphgrav_ctx *c)
 
 // ------------------------------------------------------- variant choice
 static const int kMinChunkJ = 2048;  // shortest j-chunk worth a partial slot
+// FP64 variant that recomputes the refine-listed rows (few rows per set: the
+// smallest row tile)
+static const int kRefineVariant = 0;
 
 static int ceil_log2(long long v)
 {
@@ -292,7 +311,10 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
         int v = variant_by_name(precision, it->second);
         if (v >= 0) return v;
     }
-    if (precision == SPHGRAV_FP64) return 0;
+    // FP64: two rows per thread from 2^18 on (config 2: 810 vs 754 G pairs/s,
+    // config 3: 883 vs 826), one row below (16K: 276 vs 194; the batch of
+    // 4K-131K models: 735 vs 727)
+    if (precision == SPHGRAV_FP64) return b >= 18 ? 1 : 0;
     // defaults by pair-weighted mean N = 2^b, from a sweep of single
     // polytropes on B200 (G pairs/s of the chosen shape vs the runner-up):
     //   b >= 20  W12K2Q1, 7 stages   (1M: 2027 vs 1942 for W15K1Q2)
@@ -478,6 +500,23 @@ static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_ro
     TRY(ensure(c, c->partials, (size_t)std::max(1, P.nslots) * 4 * P.itile, "partials"));
     TRY(ensure(c, c->wtile, std::max(1, P.ntiles), "wtile"));
     TRY(ensure(c, c->wdev, std::max(1, P.nsets), "W"));
+    if (P.precision == SPHGRAV_F32SPLIT && (c->refine_T > 0.0 || c->keep_scale)) {
+        TRY(ensure(c, c->gpart, (size_t)std::max(1, P.nslots) * P.itile, "error-scale partials"));
+        TRY(ensure(c, c->rcount, std::max(1, P.nsets), "refine counts"));
+        TRY(ensure(c, c->rlist, std::max(1, P.rows_tot), "refine rows"));
+        TRY(ensure(c, c->rsets, std::max(1, P.nsets), "refine sets"));
+        TRY(ensure(c, c->rnitems, 1, "refine items"));
+        TRY(ensure(c, c->rhead, 1, "refine head"));
+        const VariantInfo &V = variant_info(SPHGRAV_FP64, kRefineVariant);
+        long long tiles = 0;
+        for (const SetDesc &d : P.sets) tiles += (d.ni + V.itile() - 1) / V.itile();
+        const long long target =
+            4ll * variant_occupancy(SPHGRAV_FP64, kRefineVariant) * c->sm_count;
+        const size_t cap = (size_t)std::max(1ll, std::max(tiles, target));
+        TRY(ensure(c, c->ritems, cap, "refine items"));
+        TRY(ensure(c, c->rpart, cap * 4 * V.itile(), "refine partials"));
+        if (c->keep_scale) TRY(ensure(c, c->scale, std::max(1, P.ntot), "error scale"));
+    }
     const size_t sb = sort_temp_bytes(P.ntot, P.end_bit);
     TRY(ensure(c, c->sort_temp, std::max<size_t>(sb, 1), "sort temp"));
     if (!P.full_rows) {
@@ -517,7 +556,7 @@ static SortedF32 sorted32(sphgrav_ctx *c)
 }
 
 // The per-call pipeline on device-resident inputs and outputs.
-// Barnes-Hut mode: the preparation of the direct path (validation, Morton
+// Barnes-Hut mode: the preparation of the direct path (validation, Hilbert
 // sort, gather), then the octree, its multipoles, the group walk and the
 // scatter of the requested rows.  One particle set per call.
 static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
@@ -538,7 +577,7 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     SortedF32 F = sorted32(c);
     CUDA_TRY(launch_validate(in, n, c->err.p, st));
     CUDA_TRY(launch_bbox(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, st));
-    CUDA_TRY(launch_morton(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, P.bits, c->keys_in.p,
+    CUDA_TRY(launch_sfc_keys(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, P.bits, c->keys_in.p,
                            c->vals_in.p, st));
     CUDA_TRY(launch_sort(c->sort_temp.p, c->sort_temp.cap, c->keys_in.p, c->keys_out.p,
                          c->vals_in.p, c->vals_out.p, n, P.end_bit, st));
@@ -650,6 +689,43 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     return SPHGRAV_OK;
 }
 
+// FP64 recomputation of the rows the merge listed (split-FP32 calls): a
+// device-written plan, the FP64 kernel over it, and the scatter of the
+// refined rows over the split-FP32 ones.  No host round trip.
+static int run_refine(sphgrav_ctx *c, int nkernel, const SortedF64 &D, const OutputsDev &out)
+{
+    const Plan &P = c->plan;
+    cudaStream_t st = c->stream;
+    const int v = kRefineVariant;
+    const VariantInfo &V = variant_info(SPHGRAV_FP64, v);
+    const int resident = variant_occupancy(SPHGRAV_FP64, v) * c->sm_count;
+    CUDA_TRY(launch_refine_plan(c->sets.p, P.nsets, c->rcount.p, V.itile(), V.tj, 4 * resident,
+                                (int)std::min<size_t>(c->ritems.cap, 0x7fffffff), c->rsets.p,
+                                c->ritems.p, c->rnitems.p, c->err.p, st));
+    CUDA_TRY(cudaMemsetAsync(c->rhead.p, 0, sizeof(int), st));
+    ComputeArgs a;
+    memset(&a, 0, sizeof(a));
+    a.sets = c->rsets.p;
+    a.items = c->ritems.p;
+    a.nitems = 0;
+    a.nitems_dev = c->rnitems.p;
+    a.head = c->rhead.p;
+    a.D = D;
+    a.F = sorted32(c);
+    a.ilist = c->rlist.p;
+    a.jmeta = c->jmeta.p;
+    a.partials = c->rpart.p;
+    a.gpart = nullptr;
+    a.err = c->err.p;
+    a.nkernel = nkernel;
+    a.itile = V.itile();
+    a.band2 = 1.f;
+    CUDA_TRY(launch_compute(SPHGRAV_FP64, v, resident, a, st));
+    CUDA_TRY(launch_refine_merge(c->sets.p, c->rsets.p, c->tile_set.p, P.ntiles, P.itile, V.itile(),
+                                 c->rcount.p, c->rlist.p, D, c->rpart.p, out, st));
+    return SPHGRAV_OK;
+}
+
 static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
                       int ni, const InputsDev &in, const OutputsDev &out, double *W, int nkernel,
                       int precision)
@@ -669,7 +745,7 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     SortedF32 F = sorted32(c);
     CUDA_TRY(launch_validate(in, P.ntot, c->err.p, st));
     CUDA_TRY(launch_bbox(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, st));
-    CUDA_TRY(launch_morton(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, P.bits, c->keys_in.p,
+    CUDA_TRY(launch_sfc_keys(c->sets.p, P.nsets, P.max_n, in, c->bbox.p, P.bits, c->keys_in.p,
                            c->vals_in.p, st));
     CUDA_TRY(launch_sort(c->sort_temp.p, c->sort_temp.cap, c->keys_in.p, c->keys_out.p,
                          c->vals_in.p, c->vals_out.p, P.ntot, P.end_bit, st));
@@ -680,11 +756,11 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
         CUDA_TRY(launch_rows_range(P.sets[0], D, c->ilist.p, c->nsel.p, c->sel_temp.p,
                                    c->sel_temp.cap, st));
     }
-    if (precision == SPHGRAV_F32SPLIT) {
+    if (precision == SPHGRAV_F32SPLIT)
         CUDA_TRY(launch_itile_meta(c->sets.p, P.nsets, P.ntiles, c->tile_set.p, P.itile,
                                    c->ilist.p, D, c->imeta.p, st));
-        CUDA_TRY(launch_jmeta(c->sets.p, P.nsets, P.nmeta, c->meta_set.p, D, c->jmeta.p, st));
-    }
+    // source boxes: both kernels skip the per-pair near test on far tiles
+    CUDA_TRY(launch_jmeta(c->sets.p, P.nsets, P.nmeta, c->meta_set.p, D, c->jmeta.p, st));
     CUDA_TRY(cudaMemsetAsync(c->head.p, 0, sizeof(int), st));
     ComputeArgs a;
     a.sets = c->sets.p;
@@ -701,6 +777,10 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     a.nkernel = nkernel;
     a.itile = P.itile;
     a.band2 = (float)(c->fp64_band * c->fp64_band);
+    a.nitems_dev = nullptr;
+    const bool refine = precision == SPHGRAV_F32SPLIT && c->refine_T > 0.0;
+    const bool want_g = precision == SPHGRAV_F32SPLIT && (refine || c->keep_scale);
+    a.gpart = want_g ? c->gpart.p : nullptr;
     const bool timed = c->profiling && !c->capturing && P.nitems > 0;
     if (timed) {
         if (c->prof_used == c->prof_events.size()) {
@@ -713,8 +793,26 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     }
     if (P.nitems > 0) CUDA_TRY(launch_compute(precision, P.variant, P.grid, a, st));
     if (timed) CUDA_TRY(cudaEventRecord(c->prof_events[c->prof_used++].second, st));
+    MergeRefine R;
+    c->scale_n = 0;
+    if (want_g) {
+        R.gpart = c->gpart.p;
+        R.scale = c->keep_scale ? c->scale.p : nullptr;
+        c->scale_n = c->keep_scale ? P.ntot : 0;
+    }
+    if (refine) {
+        R.thresh2 = c->refine_T * c->refine_T;
+        R.rcount = c->rcount.p;
+        R.rlist = c->rlist.p;
+        CUDA_TRY(cudaMemsetAsync(c->rcount.p, 0, sizeof(int) * P.nsets, st));
+    }
+    c->refine_nsets = refine ? P.nsets : 0;
     CUDA_TRY(launch_merge(c->sets.p, c->tile_set.p, P.ntiles, P.itile, c->ilist.p, D,
-                          c->partials.p, out, c->wtile.p, st));
+                          c->partials.p, out, refine ? nullptr : c->wtile.p, R, st));
+    if (refine) TRY(run_refine(c, nkernel, D, out));
+    if (W && refine)
+        CUDA_TRY(launch_wtile_out(c->sets.p, c->tile_set.p, P.ntiles, P.itile, c->ilist.p, D,
+                                  out.pot, c->wtile.p, st));
     if (W) CUDA_TRY(launch_wsum(c->sets.p, P.nsets, c->wtile.p, W, st));
     return SPHGRAV_OK;
 }
@@ -946,6 +1044,9 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->imeta.release(); c->jmeta.release(); c->items.release(); c->partials.release();
     c->wtile.release(); c->wdev.release(); c->kick_counter.release(); c->probe_sink.release();
     c->range2.release();
+    c->gpart.release(); c->rcount.release(); c->rlist.release(); c->rnitems.release();
+    c->rhead.release(); c->rsets.release(); c->ritems.release(); c->rpart.release();
+    c->scale.release();
     c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release();
     c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();
     c->twsum.release(); c->tgcount.release(); c->tgflag.release(); c->tglist.release();
@@ -1360,6 +1461,52 @@ int sphgrav_set_fp64_band(sphgrav_ctx *c, double factor)
     if (!(factor >= 1.0 && factor <= 16.0))
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "fp64 band factor %g outside [1, 16]", factor);
     c->fp64_band = factor;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_set_refine(sphgrav_ctx *c, double threshold)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (!(threshold >= 0.0 && threshold <= 1e6))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "refine threshold %g outside [0, 1e6]", threshold);
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change the refine test during capture");
+    c->refine_T = threshold;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_last_refine_rows(sphgrav_ctx *c, long long *rows)
+{
+    if (!c || !rows) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL argument");
+    TRY(use_device(c));
+    *rows = 0;
+    if (c->refine_nsets <= 0) return SPHGRAV_OK;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    std::vector<int> cnt(c->refine_nsets);
+    CUDA_TRY(cudaMemcpy(cnt.data(), c->rcount.p, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost));
+    long long t = 0;
+    for (int v : cnt) t += v;
+    *rows = t;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_keep_error_scale(sphgrav_ctx *c, int on)
+{
+    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change this during capture");
+    c->keep_scale = on != 0;
+    if (!c->keep_scale) c->scale_n = 0;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_error_scale(sphgrav_ctx *c, int n, double *G)
+{
+    if (!c || (n > 0 && !G)) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n != c->scale_n)
+        return set_err(SPHGRAV_ERR_PROTOCOL,
+                       "no error scale of %d rows kept (last split-FP32 call kept %d)", n, c->scale_n);
+    TRY(use_device(c));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (n > 0) CUDA_TRY(cudaMemcpy(G, c->scale.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return SPHGRAV_OK;
 }
 

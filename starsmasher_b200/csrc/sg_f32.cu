@@ -268,6 +268,12 @@ struct WsSmem {
     static constexpr uint32_t TX = RAWSTAGE + NMETA * 32;  // bytes per tile
 };
 
+// Rows farther than SHIFT_H * H from their i-tile centre are listed for the
+// FP64 refine (measured on the collision sweep: the coordinate shift stays
+// below 1.3e-7 relative for |x'| < 8 H, reaches ~1e-6 beyond 24 H; 0-0.3% of
+// the rows of the benchmark workloads lie beyond 8 H).
+constexpr float SHIFT_H = 8.f;
+
 template <int W, int K, int Q, int TJ, int NS, bool NEWTON>
 __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 {
@@ -304,6 +310,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     const int grp = lane / Q, phase = lane % Q;
     const SortedF64 D = a.D;
     const SortedF32 F = a.F;
+    const int nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
 
     if (tid == 0) {
         for (int s = 0; s < NS; s++) {
@@ -348,7 +355,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
         if (tid == 0) s_item[iter & 1] = atomicAdd(a.head, 1);
         if (__syncthreads_or(failed)) break;
         const int it = s_item[iter & 1];
-        if (it >= a.nitems) break;
+        if (it >= nitems) break;
         const WorkItem Wk = a.items[it];
         const SetDesc S = a.sets[Wk.set];
         const ITileMeta C = a.imeta[S.tile_off + Wk.tile];
@@ -429,6 +436,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
             int ip[K];
             bool act[K];
             f2 xi[K], yi[K], zi[K];
+            f2 g2[K];  // sum over tiles of |FP32 tile sum|^2 per packed lane (error scale)
+            bool shifted[K];  // row far from the i-tile centre (see below)
             float h2i[K];
             float wlo[3] = {INFINITY, INFINITY, INFINITY};
             float whi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -461,6 +470,14 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                 yi[k] = pk(y, y);
                 zi[k] = pk(z, z);
                 h2i[k] = h2;
+                g2[k] = pk(0.f, 0.f);
+                // The FP32 rounding of a row's tile-relative coordinate shifts the
+                // row by up to ~1e-7 |x'|, a coherent error (tidal field times the
+                // shift) that grows with |x'| / H; i-tiles whose rows span a
+                // space-filling-curve exit leave a few rows tens of H from the
+                // centre.  Such rows (|x'| > SHIFT_H H) get an infinite error
+                // scale, so the refine recomputes them in FP64.
+                shifted[k] = act[k] && x * x + y * y + z * z > SHIFT_H * SHIFT_H * F.h2[ip[k]];
 #pragma unroll
                 for (int c = 0; c < 8; c++) s_acc[(k * 8 + c) * NT + tid] = 0.f;
             }
@@ -595,6 +612,9 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     }
 #pragma unroll
                     for (int k = 0; k < K; k++) {
+                        g2[k] = fma2(tx[k], tx[k], g2[k]);
+                        g2[k] = fma2(ty[k], ty[k], g2[k]);
+                        g2[k] = fma2(tz[k], tz[k], g2[k]);
                         float *acc = s_acc + (k * 8) * NT + tid;
                         fold(acc, acc + 4 * NT, tx[k]);
                         fold(acc + NT, acc + 5 * NT, ty[k]);
@@ -616,8 +636,21 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
             if (!failed) {
                 // combine the Q threads of a row (fixed order), convert, write FP64 partials
                 __syncwarp();
-                double *p = a.partials +
-                            (size_t)(S.slot_off + Wk.tile * S.nchunks + Wk.chunk) * 4 * ITILE;
+                const size_t slot = (size_t)(S.slot_off + Wk.tile * S.nchunks + Wk.chunk);
+                double *p = a.partials + slot * 4 * ITILE;
+                if (a.gpart) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        float ga, gb;
+                        upk(g2[k], ga, gb);
+                        float gs = ga + gb;
+#pragma unroll
+                        for (int o = 1; o < Q; o <<= 1) gs += __shfl_xor_sync(0xffffffffu, gs, o);
+                        if (phase == 0 && act[k])
+                            a.gpart[slot * ITILE + warp * RPW * K + k * RPW + grp] =
+                                shifted[k] ? INFINITY : gs * (SA * SA);
+                    }
+                }
                 if (phase == 0) {
 #pragma unroll
                     for (int k = 0; k < K; k++) {

@@ -5,43 +5,105 @@
 // r^2 >= max(H_i^2, H_j^2), otherwise the softened pair of pair_f64_slots.
 // Work decomposition (persistent CTAs over a device queue of
 // (set, i-tile, j-chunk) items):
-//   * K rows per thread kept in registers, NT threads per CTA;
-//   * j-tiles of TJ particles staged in shared memory as SoA doubles
-//     (x, y, z, m, H^2), the next tile prefetched into registers while the
-//     current one is summed;
+//   * K rows per thread kept in registers (a warp owns 32 K consecutive
+//     sorted rows, so its rows form a compact box), NT threads per CTA;
+//   * j-tiles of TJ sources staged in shared memory as SoA doubles
+//     (x, y, z, m, H^2) by 1-D bulk async copies (cp.async.bulk, the TMA
+//     engine; no multicast) into an NS-stage ring completing on mbarriers,
+//     together with the tile's bounding-box records;
+//   * per (warp, tile) a box test: when every pair of the warp's rows with
+//     the tile's sources is Newtonian (r^2 > max H^2 for all of them), the
+//     tile runs a loop without the per-pair branch;
 //   * one FP64 partial sum per (row, j-chunk), merged in chunk order by
 //     k_merge.
+// Far pairs take 1/r from the PTX rsqrt.approx.ftz.f64 seed y0 refined by one
+// third-order step of the series (1 - e)^(-1/2) = 1 + e/2 + 3e^2/8 + O(e^3),
+// e = 1 - r^2 y0^2 (Householder's method for x^(-1/2)): 5 FP64 operations
+// to full precision.
 #include "sg_launch.h"
 
 namespace sg {
 
-template <int NT, int K, int TJ>
+__device__ __forceinline__ double rsqrt_approx_f64(double x)
+{
+    double r;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    return r;
+}
+
+// 1/sqrt(r2) for r2 > 0 (normal range): seed and one third-order correction.
+__device__ __forceinline__ double rsqrt_f64(double r2)
+{
+    const double y0 = rsqrt_approx_f64(r2);
+    const double e = fma(-(r2 * y0), y0, 1.0);
+    const double q = e * fma(e, 0.375, 0.5);
+    return fma(y0, q, y0);
+}
+
+template <int NT, int K, int TJ, int NS>
 __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
 {
-    static_assert(TJ % NT == 0, "j-tile must be a multiple of the block");
+    static_assert(TJ % META_J == 0, "j-tile must hold whole metadata records");
     constexpr int ITILE = NT * K;
-    constexpr int LPT = TJ / NT;  // j loads per thread per tile
-    __shared__ double s_x[TJ], s_y[TJ], s_z[TJ], s_m[TJ], s_h[TJ];
+    constexpr int NMETA = TJ / META_J;
+    constexpr uint32_t TX = 5 * TJ * 8 + NMETA * (uint32_t)sizeof(JMeta);
+    constexpr uint32_t WAIT_LIMIT = 1u << 22;
+    __shared__ __align__(128) double s_src[NS][5][TJ];  // x y z m H^2
+    __shared__ __align__(16) JMeta s_meta[NS][NMETA];
+    __shared__ __align__(8) uint64_t s_bar[NS];
     __shared__ int s_item;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const SortedF64 D = a.D;
+    const int nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; s++) mbar_init(&s_bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    uint32_t g = 0;          // tiles this CTA has passed through its ring
+    bool failed = false;
+    bool pending[NS];        // thread 0: copies in flight per stage ...
+    uint32_t pend_par[NS];   // ... and the phase they complete
+#pragma unroll
+    for (int s = 0; s < NS; s++) { pending[s] = false; pend_par[s] = 0u; }
+
+    // bulk copies of set-local sorted slots [jt, jt + TJ) into stage gt % NS
+    auto issue = [&](const SetDesc &S, int jt, uint32_t gt) {
+        const int b = gt % NS;
+        const int s0 = S.poff + jt;
+        pending[b] = true;
+        pend_par[b] = (gt / NS) & 1;
+        fence_mbar_init();  // earlier generic reads of the stage before the async writes
+        mbar_arrive_expect_tx(&s_bar[b], TX);
+        const double *src[5] = {D.x, D.y, D.z, D.m, D.h2};
+#pragma unroll
+        for (int q = 0; q < 5; q++) bulk_g2s(s_src[b][q], src[q] + s0, TJ * 8, &s_bar[b]);
+        bulk_g2s(s_meta[b], a.jmeta + S.meta_off + jt / META_J, NMETA * (uint32_t)sizeof(JMeta),
+                 &s_bar[b]);
+    };
 
     for (;;) {
         if (tid == 0) s_item = atomicAdd(a.head, 1);
-        __syncthreads();
+        if (__syncthreads_or(failed)) break;
         const int it = s_item;
-        __syncthreads();
-        if (it >= a.nitems) break;
+        if (it >= nitems) break;
         const WorkItem W = a.items[it];
         const SetDesc S = a.sets[W.set];
+        const int ntile = (W.je - W.jb) / TJ;
+        if (tid == 0)
+            for (int t = 0; t < NS && t < ntile; t++) issue(S, W.jb + t * TJ, g + t);
 
         int ip[K];
         bool act[K];
         double xi[K], yi[K], zi[K], hi2[K];
         double ax[K], ay[K], az[K], pot[K];
+        double wlo[3] = {INFINITY, INFINITY, INFINITY}, whi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        double wh2 = 0.0;
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            const int r = W.tile * ITILE + k * NT + tid;
+            const int r = W.tile * ITILE + warp * 32 * K + k * 32 + lane;
             act[k] = r < S.ni;
             ip[k] = act[k] ? a.ilist[S.ioff + r] : -1;
             xi[k] = act[k] ? D.x[ip[k]] : FAR_POS;
@@ -49,63 +111,107 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
             zi[k] = act[k] ? D.z[ip[k]] : -FAR_POS;
             hi2[k] = act[k] ? D.h2[ip[k]] : 0.0;
             ax[k] = ay[k] = az[k] = pot[k] = 0.0;
+            if (act[k]) {
+                wlo[0] = fmin(wlo[0], xi[k]); whi[0] = fmax(whi[0], xi[k]);
+                wlo[1] = fmin(wlo[1], yi[k]); whi[1] = fmax(whi[1], yi[k]);
+                wlo[2] = fmin(wlo[2], zi[k]); whi[2] = fmax(whi[2], zi[k]);
+                wh2 = fmax(wh2, hi2[k]);
+            }
         }
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            for (int o = 16; o > 0; o >>= 1) {
+                wlo[d] = fmin(wlo[d], __shfl_xor_sync(0xffffffffu, wlo[d], o));
+                whi[d] = fmax(whi[d], __shfl_xor_sync(0xffffffffu, whi[d], o));
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) wh2 = fmax(wh2, __shfl_xor_sync(0xffffffffu, wh2, o));
+        const bool warp_rows = wlo[0] <= whi[0];
 
-        // register prefetch of the first tile
-        double px[LPT], py[LPT], pz[LPT], pm[LPT], ph[LPT];
+        for (int t = 0; t < ntile; t++) {
+            const uint32_t gt = g + t;
+            const int s = gt % NS;
+            const bool ok = mbar_wait_bounded(&s_bar[s], (gt / NS) & 1, WAIT_LIMIT);
+            if (ok && tid == 0) pending[s] = false;
+            if (ok && warp_rows) {
+                const double *sx = s_src[s][0], *sy = s_src[s][1], *sz = s_src[s][2];
+                const double *sm = s_src[s][3], *sh = s_src[s][4];
+                // box test: the gap between the warp's rows and each record's
+                // box bounds r from below; far when it exceeds every H
+                bool far = true;
 #pragma unroll
-        for (int l = 0; l < LPT; l++) {
-            const int slot = S.poff + W.jb + l * NT + tid;
-            px[l] = D.x[slot]; py[l] = D.y[slot]; pz[l] = D.z[slot];
-            pm[l] = D.m[slot]; ph[l] = D.h2[slot];
-        }
-        for (int jt = W.jb; jt < W.je; jt += TJ) {
+                for (int r = 0; r < NMETA; r++) {
+                    const JMeta M = s_meta[s][r];
+                    if (M.ex < 0.f) continue;  // no particle
+                    const double c[3] = {M.cx, M.cy, M.cz}, e[3] = {M.ex, M.ey, M.ez};
+                    double d2 = 0.0;
 #pragma unroll
-            for (int l = 0; l < LPT; l++) {
-                const int t = l * NT + tid;
-                s_x[t] = px[l]; s_y[t] = py[l]; s_z[t] = pz[l]; s_m[t] = pm[l]; s_h[t] = ph[l];
-            }
-            __syncthreads();
-            if (jt + TJ < W.je) {
-#pragma unroll
-                for (int l = 0; l < LPT; l++) {
-                    const int slot = S.poff + jt + TJ + l * NT + tid;
-                    px[l] = D.x[slot]; py[l] = D.y[slot]; pz[l] = D.z[slot];
-                    pm[l] = D.m[slot]; ph[l] = D.h2[slot];
+                    for (int d = 0; d < 3; d++) {
+                        const double gap = fmax(0.0, fmax((c[d] - e[d]) - whi[d], wlo[d] - (c[d] + e[d])));
+                        d2 = fma(gap, gap, d2);
+                    }
+                    far = far && d2 * (1.0 - 1e-12) > fmax(wh2, (double)M.h2max);
                 }
-            }
+                if (far) {
 #pragma unroll 2
-            for (int j = 0; j < TJ; j++) {
-                const double xj = s_x[j], yj = s_y[j], zj = s_z[j], mj = s_m[j], hj = s_h[j];
+                    for (int j = 0; j < TJ; j++) {
+                        const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
 #pragma unroll
-                for (int k = 0; k < K; k++) {
-                    const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
-                    const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-                    if (r2 >= fmax(hi2[k], hj)) {
-                        const double rinv = rsqrt(r2);
-                        const double mr = mj * rinv;
-                        const double mr3 = mr * rinv * rinv;
-                        ax[k] = fma(mr3, dx, ax[k]);
-                        ay[k] = fma(mr3, dy, ay[k]);
-                        az[k] = fma(mr3, dz, az[k]);
-                        pot[k] -= mr;
-                    } else if (act[k]) {
-                        const PairOut o = pair_f64_slots(D, a.nkernel, ip[k], S.poff + jt + j);
-                        ax[k] += o.ax;
-                        ay[k] += o.ay;
-                        az[k] += o.az;
-                        pot[k] += o.pot;
+                        for (int k = 0; k < K; k++) {
+                            const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
+                            const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+                            const double y = rsqrt_f64(r2);
+                            const double mr = mj * y;
+                            const double mr3 = mr * (y * y);
+                            ax[k] = fma(mr3, dx, ax[k]);
+                            ay[k] = fma(mr3, dy, ay[k]);
+                            az[k] = fma(mr3, dz, az[k]);
+                            pot[k] -= mr;
+                        }
+                    }
+                } else {
+                    const int jt = W.jb + t * TJ;
+                    for (int j = 0; j < TJ; j++) {
+                        const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j], hj = sh[j];
+#pragma unroll
+                        for (int k = 0; k < K; k++) {
+                            const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
+                            const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+                            if (r2 >= fmax(hi2[k], hj)) {
+                                const double y = rsqrt_f64(r2);
+                                const double mr = mj * y;
+                                const double mr3 = mr * (y * y);
+                                ax[k] = fma(mr3, dx, ax[k]);
+                                ay[k] = fma(mr3, dy, ay[k]);
+                                az[k] = fma(mr3, dz, az[k]);
+                                pot[k] -= mr;
+                            } else if (act[k]) {
+                                const PairOut o = pair_f64_slots(D, a.nkernel, ip[k], S.poff + jt + j);
+                                ax[k] += o.ax;
+                                ay[k] += o.ay;
+                                az[k] += o.az;
+                                pot[k] += o.pot;
+                            }
+                        }
                     }
                 }
             }
-            __syncthreads();
+            // every thread is done with stage s (or a wait gave up)
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicOr(a.err, DEVERR_TIMEOUT);
+                failed = true;
+                break;
+            }
+            if (tid == 0 && t + NS < ntile) issue(S, W.jb + (t + NS) * TJ, gt + NS);
         }
+        g += ntile;
+        if (failed) break;
 
         double *p = a.partials + (size_t)(S.slot_off + W.tile * S.nchunks + W.chunk) * 4 * ITILE;
 #pragma unroll
         for (int k = 0; k < K; k++) {
             if (act[k]) {
-                const int li = k * NT + tid;
+                const int li = warp * 32 * K + k * 32 + lane;
                 p[li] = ax[k];
                 p[ITILE + li] = ay[k];
                 p[2 * ITILE + li] = az[k];
@@ -113,18 +219,27 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
             }
         }
     }
+    // never leave with bulk copies in flight into this CTA's shared memory
+    if (tid == 0) {
+        for (int b = 0; b < NS; b++)
+            if (pending[b]) mbar_wait_bounded(&s_bar[b], pend_par[b], WAIT_LIMIT);
+    }
 }
 
-static const VariantInfo kF64Variants[] = {
-    {0, 128, 1, 1, 128, 0, "fp64_nt128_k1_tj128", 128},
-    {0, 256, 1, 1, 256, 0, "fp64_nt256_k1_tj256", 256},
-    {0, 128, 2, 1, 128, 0, "fp64_nt128_k2_tj128", 256},
-};
-static const void *kF64Kernels[] = {
-    (const void *)k_fp64<128, 1, 128>,
-    (const void *)k_fp64<256, 1, 256>,
-    (const void *)k_fp64<128, 2, 128>,
-};
+// name, threads NT, rows per thread K, j-tile TJ, stages NS.  Variant 0 (the
+// smallest row tile) also recomputes the split-FP32 refine rows.
+#define SG_F64_VARIANTS(X)                          \
+    X(128, 1, 128, 3, "fp64_nt128_k1_tj128")        \
+    X(128, 2, 128, 3, "fp64_nt128_k2_tj128")        \
+    X(128, 4, 128, 3, "fp64_nt128_k4_tj128")        \
+    X(256, 1, 128, 3, "fp64_nt256_k1_tj128")
+
+#define SG_INFO(NT, K, TJ, NS, NAME) {0, NT, K, 1, TJ, 0, NAME, NT * K},
+static const VariantInfo kF64Variants[] = {SG_F64_VARIANTS(SG_INFO)};
+#undef SG_INFO
+#define SG_PTR(NT, K, TJ, NS, NAME) (const void *)k_fp64<NT, K, TJ, NS>,
+static const void *kF64Kernels[] = {SG_F64_VARIANTS(SG_PTR)};
+#undef SG_PTR
 constexpr int kNF64 = sizeof(kF64Variants) / sizeof(kF64Variants[0]);
 
 int f64_variant_count() { return kNF64; }
@@ -133,14 +248,17 @@ const void *f64_kernel(int v) { return kF64Kernels[v]; }
 
 cudaError_t launch_f64(int v, int grid, const ComputeArgs &a, cudaStream_t st)
 {
-    switch (v) {
-    case 0: k_fp64<128, 1, 128><<<grid, 128, 0, st>>>(a); break;
-    case 1: k_fp64<256, 1, 256><<<grid, 256, 0, st>>>(a); break;
-    case 2: k_fp64<128, 2, 128><<<grid, 128, 0, st>>>(a); break;
-    default: return cudaErrorInvalidValue;
-    }
-    ++g_launches;
-    return cudaGetLastError();
+    int idx = 0;
+#define SG_CASE(NT, K, TJ, NS, NAME)                               \
+    if (v == idx) {                                                \
+        k_fp64<NT, K, TJ, NS><<<grid, NT, 0, st>>>(a);             \
+        ++g_launches;                                              \
+        return cudaGetLastError();                                 \
+    }                                                              \
+    ++idx;
+    SG_F64_VARIANTS(SG_CASE)
+#undef SG_CASE
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace sg

@@ -3,11 +3,14 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include <atomic>
 #include "sg_internal.cuh"
 
 namespace sg {
 
-extern unsigned long long g_launches;  // kernels launched by the library
+// Kernels launched by the library; atomic because entry points on different
+// contexts (or the allocation-free one) may run on several host threads.
+extern std::atomic<unsigned long long> g_launches;
 
 // Input arrays in the caller's (original) order, device pointers.
 struct InputsDev {
@@ -22,7 +25,7 @@ struct OutputsDev {
 cudaError_t launch_validate(const InputsDev &in, int ntot, int *err, cudaStream_t st);
 cudaError_t launch_bbox(const SetDesc *sets, int nsets, int max_n, const InputsDev &in,
                         unsigned long long *bbox /* 6 per set */, cudaStream_t st);
-cudaError_t launch_morton(const SetDesc *sets, int nsets, int max_n, const InputsDev &in,
+cudaError_t launch_sfc_keys(const SetDesc *sets, int nsets, int max_n, const InputsDev &in,
                           const unsigned long long *bbox, int bits_per_axis,
                           unsigned long long *keys, int *vals, cudaStream_t st);
 size_t sort_temp_bytes(int ntot, int end_bit);
@@ -56,6 +59,13 @@ struct ComputeArgs {
     const ITileMeta *imeta;
     const JMeta *jmeta;
     double *partials;    // [slot][4][itile]
+    // split-FP32: [slot][itile] sum over the item's j-tiles of |FP32 tile sum|^2
+    // (acceleration components, both packed lanes): the scale of the FP32
+    // rounding error of the row, merged into the refine test (nullable)
+    float *gpart;
+    // when non-null the item count is read here instead of `nitems` (work
+    // lists planned on the device, e.g. the FP64 refine of flagged rows)
+    const int *nitems_dev;
     int *err;
     int nkernel;
     int itile;
@@ -80,9 +90,42 @@ int variant_occupancy(int precision, int v);
 cudaError_t launch_compute(int precision, int v, int grid, const ComputeArgs &a, cudaStream_t st);
 
 // --- merge and diagnostics (sg_prep.cu)
+// Refine test of the merge (split-FP32 calls): rows whose error scale G^2
+// exceeds thresh2 * |a|^2 are listed for the FP64 refine.
+struct MergeRefine {
+    const float *gpart = nullptr;  // [slot][itile] G^2 partials; null: no test
+    double thresh2 = 0.0;          // T^2
+    int *rcount = nullptr;         // [nsets] rows listed per set (zeroed before the merge)
+    int *rlist = nullptr;          // listed sorted slots; set s at [S.ioff, S.ioff + S.ni)
+    double *scale = nullptr;       // optional: G per row in the caller's order
+};
 cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, int ntiles_total, int itile,
                          const int *ilist, const SortedF64 D, const double *partials,
-                         OutputsDev out, double *wtile, cudaStream_t st);
+                         OutputsDev out, double *wtile, const MergeRefine &R, cudaStream_t st);
+cudaError_t launch_wtile_out(const SetDesc *sets, const int *tile_set, int ntiles_total, int itile,
+                             const int *ilist, const SortedF64 D, const double *pot, double *wtile,
+                             cudaStream_t st);
+
+// --- FP64 refine of the listed rows (sg_refine.cu)
+// Plans the refine on the device from the per-set counts: for set s the rows
+// rlist[S.ioff, S.ioff + rcount[s]) in tiles of `itile` rows, every tile
+// split into the same number of j-chunks (enough items to fill `target`
+// persistent blocks, at least 1024 sources per chunk), one partial slot per
+// item.  Writes rsets (copies of sets with ni, ntiles, nchunks, slot_off of
+// the refine), the items and their count.  At most max_items items are
+// written; a plan that would need more sets DEVERR_INPUT (never expected:
+// the host sizes max_items for every row flagged).
+cudaError_t launch_refine_plan(const SetDesc *sets, int nsets, const int *rcount, int itile,
+                               int tj, int target, int max_items, SetDesc *rsets,
+                               WorkItem *items, int *nitems, int *err, cudaStream_t st);
+// Scatter the refined rows: chunk sums in chunk order, written over the
+// split-FP32 results in the caller's order.  Launched over the main plan's
+// tiles (grid ntiles_main); tile t covers refine-list entries
+// [lt * itile_main, (lt + 1) * itile_main) of its set.
+cudaError_t launch_refine_merge(const SetDesc *sets, const SetDesc *rsets, const int *tile_set,
+                                int ntiles_main, int itile_main, int itile_ref, const int *rcount,
+                                const int *rlist, const SortedF64 D, const double *rpart,
+                                OutputsDev out, cudaStream_t st);
 cudaError_t launch_wsum(const SetDesc *sets, int nsets, const double *wtile, double *W,
                         cudaStream_t st);
 cudaError_t launch_range2(int n, const double *hp, const double *u, double *range2, cudaStream_t st);
@@ -94,7 +137,7 @@ cudaError_t launch_wait_selftest(uint32_t polls, int *err, cudaStream_t st);
 
 // --- Barnes-Hut octree (sg_tree.cu)
 constexpr int TREE_LEAF = 16;    // a node with more particles splits
-constexpr int TREE_LEVELS = 21;  // Morton bits per axis
+constexpr int TREE_LEVELS = 21;  // key bits per axis (one octree level per 3-bit digit)
 // device level table: [L] first node of level L (L = 0..TREE_LEVELS + 1), then a
 // node-capacity overflow flag
 constexpr int TREE_LV_OVERFLOW = TREE_LEVELS + 2;
@@ -134,7 +177,7 @@ struct NodeMP {        // multipoles (64 bytes)
 };
 struct TreeBuildArgs {
     int n;
-    const unsigned long long *keys;  // sorted Morton keys of the n particles
+    const unsigned long long *keys;  // sorted Hilbert keys of the n particles
     TreeNode *nodes;
     int cap;                         // node capacity
     int *cnt, *off;                  // per-level scratch (n + 1 entries)

@@ -139,8 +139,10 @@ __global__ void k_merge_noalloc(int n, int nchunks, const double *part, double *
 
 using namespace sg;
 
-// Device address of the static scratch, looked up once per device.
-static void *g_noalloc_ptr[64] = {nullptr};
+// Device address of the static scratch, looked up once per device.  Atomic:
+// host threads calling on different devices (or racing on the first call of
+// one device, which both resolve to the same address) must not race.
+static std::atomic<void *> g_noalloc_ptr[64];
 
 extern "C" int sphgrav_forces_fp64_noalloc(int n, const double *x, const double *y,
                                            const double *z, const double *mass,
@@ -157,7 +159,8 @@ extern "C" int sphgrav_forces_fp64_noalloc(int n, const double *x, const double 
         cudaGetLastError();
         return SPHGRAV_ERR_NO_DEVICE;
     }
-    if (!g_noalloc_ptr[dev]) {
+    void *part_p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!part_p) {
         // set-up on this device's first call (host code cannot use the
         // symbol's name as a device address)
         void *p = nullptr;
@@ -166,9 +169,10 @@ extern "C" int sphgrav_forces_fp64_noalloc(int n, const double *x, const double 
             cudaGetLastError();
             return SPHGRAV_ERR_CUDA;
         }
-        g_noalloc_ptr[dev] = p;
+        g_noalloc_ptr[dev].store(p, std::memory_order_release);
+        part_p = p;
     }
-    double *part = (double *)g_noalloc_ptr[dev];
+    double *part = (double *)part_p;
     // j-chunks: enough blocks to fill the GPU at small n, within the scratch
     const long long per_chunk = 4ll * n;
     int nchunks = (int)std::min<long long>(16, (long long)NA_SCRATCH_DOUBLES / per_chunk);

@@ -3,9 +3,14 @@
 // kick kernel of device-resident sweeps.
 //
 // Layout produced per call (all on the device):
-//   * per-set bounding boxes -> 3 x bits Morton keys with the set index above
-//     them -> one radix sort of all particles: particles of a set stay
-//     contiguous and in set order, spatially sorted inside the set;
+//   * per-set bounding boxes -> 3 x bits Hilbert-curve keys with the set
+//     index above them -> one radix sort of all particles: particles of a
+//     set stay contiguous and in set order, spatially sorted inside the set
+//     along a Hilbert curve (consecutive cells are face neighbours, so every
+//     run of consecutive particles -- an i-tile, a j-tile -- is spatially
+//     compact; a Morton order jumps across octant boundaries, and an i-tile
+//     across such a jump put rows far from the tile centre, where the FP32
+//     rounding of their tile-relative coordinates shifted them measurably);
 //   * padded sorted SoA arrays (each set padded to a multiple of PAD_J with
 //     mass-0 slots far away): FP64 copies for the FP64 kernel and the
 //     near-field pairs, FP32 hi+lo position pairs for the split kernel;
@@ -16,7 +21,7 @@
 
 namespace sg {
 
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
 
 static inline unsigned grid_for(long long n, int block, int cap)
 {
@@ -96,7 +101,7 @@ cudaError_t launch_bbox(const SetDesc *sets, int nsets, int max_n, const InputsD
     return cudaGetLastError();
 }
 
-// ------------------------------------------------------------ Morton keys
+// ----------------------------------------------------------- Hilbert keys
 __device__ __forceinline__ unsigned long long spread3(unsigned long long v)
 {
     v &= 0x1fffffull;
@@ -108,8 +113,43 @@ __device__ __forceinline__ unsigned long long spread3(unsigned long long v)
     return v;
 }
 
-__global__ void k_morton(const SetDesc *sets, InputsDev in, const unsigned long long *bbox,
-                         int bits, unsigned long long *keys, int *vals)
+// Index of cell (x0, x1, x2) (bits per axis) on the 3-D Hilbert curve, after
+// J. Skilling, "Programming the Hilbert curve", AIP Conf. Proc. 707 (2004):
+// the axes are transformed in place (undo the excess work of the inverse
+// map, then Gray-encode) and the transposed form is interleaved into the
+// index.  The top 3 L bits of the index name the level-L octree cell, as
+// those of a Morton key do, so cells are contiguous key ranges.
+__device__ __forceinline__ unsigned long long hilbert3(unsigned x0, unsigned x1, unsigned x2,
+                                                       int bits)
+{
+    unsigned X[3] = {x0, x1, x2};
+    const unsigned M = 1u << (bits - 1);
+    for (unsigned Q = M; Q > 1; Q >>= 1) {
+        const unsigned P = Q - 1;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            if (X[i] & Q) {
+                X[0] ^= P;
+            } else {
+                const unsigned t = (X[0] ^ X[i]) & P;
+                X[0] ^= t;
+                X[i] ^= t;
+            }
+        }
+    }
+    X[1] ^= X[0];
+    X[2] ^= X[1];
+    unsigned t = 0;
+    for (unsigned Q = M; Q > 1; Q >>= 1)
+        if (X[2] & Q) t ^= Q - 1;
+    X[0] ^= t;
+    X[1] ^= t;
+    X[2] ^= t;
+    return (spread3(X[0]) << 2) | (spread3(X[1]) << 1) | spread3(X[2]);
+}
+
+__global__ void k_sfc_keys(const SetDesc *sets, InputsDev in, const unsigned long long *bbox,
+                           int bits, unsigned long long *keys, int *vals)
 {
     const int s = blockIdx.y;
     const SetDesc S = sets[s];
@@ -125,24 +165,23 @@ __global__ void k_morton(const SetDesc *sets, InputsDev in, const unsigned long 
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S.n; k += gridDim.x * blockDim.x) {
         const int p = S.off + k;
         const double v[3] = {in.x[p], in.y[p], in.z[p]};
-        unsigned long long code = 0;
+        unsigned q[3];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             double c = (v[d] - lo[d]) * scale[d];
-            c = fmin(fmax(c, 0.0), cells);
-            code |= spread3((unsigned long long)c) << (2 - d);
+            q[d] = (unsigned)fmin(fmax(c, 0.0), cells);
         }
-        keys[p] = ((unsigned long long)s << (3 * bits)) | code;
+        keys[p] = ((unsigned long long)s << (3 * bits)) | hilbert3(q[0], q[1], q[2], bits);
         vals[p] = p;
     }
 }
 
-cudaError_t launch_morton(const SetDesc *sets, int nsets, int max_n, const InputsDev &in,
+cudaError_t launch_sfc_keys(const SetDesc *sets, int nsets, int max_n, const InputsDev &in,
                           const unsigned long long *bbox, int bits_per_axis,
                           unsigned long long *keys, int *vals, cudaStream_t st)
 {
     dim3 grid(grid_for(max_n, 256, 1024), nsets);
-    k_morton<<<grid, 256, 0, st>>>(sets, in, bbox, bits_per_axis, keys, vals);
+    k_sfc_keys<<<grid, 256, 0, st>>>(sets, in, bbox, bits_per_axis, keys, vals);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -401,24 +440,46 @@ cudaError_t launch_jmeta(const SetDesc *sets, int nsets, int nmeta_total, const 
 }
 
 // ------------------------------------------------------------------ merge
+// Block-wide sum of one double per thread in a fixed order (tree over the
+// thread index); the result is valid in thread 0.
+__device__ double block_sum_fixed(double w)
+{
+    __shared__ double s_w[1024];
+    s_w[threadIdx.x] = w;
+    __syncthreads();
+    for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s_w[threadIdx.x] += s_w[threadIdx.x + o];
+        __syncthreads();
+    }
+    return s_w[0];
+}
+
 // Ordered second pass: row sums over the j-chunks in chunk order (the result
 // does not depend on which block computed which chunk), scatter to the
 // caller's order, and the per-tile sum of m_i * phi_i in a fixed order.
+// Split-FP32 calls also merge the rows' error scales G^2 (sum over j-tiles of
+// |FP32 tile sum|^2) and append every row with G^2 > thresh2 |a|^2 to its
+// set's refine list, rlist[S.ioff + k], k counted in rcount[set].
 __global__ void k_merge(const SetDesc *sets, const int *tile_set, int itile, const int *ilist,
-                        SortedF64 D, const double *partials, OutputsDev out, double *wtile)
+                        SortedF64 D, const double *partials, OutputsDev out, double *wtile,
+                        MergeRefine R)
 {
     const int t = blockIdx.x;
-    const SetDesc S = sets[tile_set[t]];
+    const int set = tile_set[t];
+    const SetDesc S = sets[set];
     const int lt = t - S.tile_off;
     const int r0 = lt * itile;
     const int nrow = min(itile, S.ni - r0);
     double w = 0.0;
     for (int li = threadIdx.x; li < nrow; li += blockDim.x) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        float g2 = 0.f;
         for (int c = 0; c < S.nchunks; c++) {
-            const double *p = partials + (size_t)(S.slot_off + lt * S.nchunks + c) * 4 * itile;
+            const size_t slot = (size_t)(S.slot_off + lt * S.nchunks + c);
+            const double *p = partials + slot * 4 * itile;
 #pragma unroll
             for (int q = 0; q < 4; q++) acc[q] += p[q * itile + li];
+            if (R.gpart) g2 += R.gpart[slot * itile + li];
         }
         const int slot = ilist[S.ioff + r0 + li];
         const int o = D.orig[slot];
@@ -427,23 +488,54 @@ __global__ void k_merge(const SetDesc *sets, const int *tile_set, int itile, con
         out.az[o] = acc[2];
         out.pot[o] = acc[3];
         w += D.m[slot] * acc[3];
+        if (R.gpart) {
+            const double a2 = acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2];
+            if (R.rlist && (double)g2 > R.thresh2 * a2) {
+                const int k = atomicAdd(&R.rcount[set], 1);
+                R.rlist[S.ioff + k] = slot;
+            }
+            if (R.scale) R.scale[o] = sqrt((double)g2);
+        }
     }
-    __shared__ double s_w[1024];
-    s_w[threadIdx.x] = w;
-    __syncthreads();
-    for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
-        if (threadIdx.x < o) s_w[threadIdx.x] += s_w[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0 && wtile) wtile[t] = s_w[0];
+    const double wt = block_sum_fixed(w);
+    if (threadIdx.x == 0 && wtile) wtile[t] = wt;
 }
 
 cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, int ntiles_total, int itile,
                          const int *ilist, const SortedF64 D, const double *partials,
-                         OutputsDev out, double *wtile, cudaStream_t st)
+                         OutputsDev out, double *wtile, const MergeRefine &R, cudaStream_t st)
 {
     if (ntiles_total <= 0) return cudaSuccess;
-    k_merge<<<ntiles_total, 256, 0, st>>>(sets, tile_set, itile, ilist, D, partials, out, wtile);
+    k_merge<<<ntiles_total, 256, 0, st>>>(sets, tile_set, itile, ilist, D, partials, out, wtile, R);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+// Per-tile sum of m_i * phi_i from the outputs (caller order), in the order of
+// k_merge; used after rows were replaced by the FP64 refine.
+__global__ void k_wtile_out(const SetDesc *sets, const int *tile_set, int itile, const int *ilist,
+                            SortedF64 D, const double *pot, double *wtile)
+{
+    const int t = blockIdx.x;
+    const SetDesc S = sets[tile_set[t]];
+    const int lt = t - S.tile_off;
+    const int r0 = lt * itile;
+    const int nrow = min(itile, S.ni - r0);
+    double w = 0.0;
+    for (int li = threadIdx.x; li < nrow; li += blockDim.x) {
+        const int slot = ilist[S.ioff + r0 + li];
+        w += D.m[slot] * pot[D.orig[slot]];
+    }
+    const double wt = block_sum_fixed(w);
+    if (threadIdx.x == 0) wtile[t] = wt;
+}
+
+cudaError_t launch_wtile_out(const SetDesc *sets, const int *tile_set, int ntiles_total, int itile,
+                             const int *ilist, const SortedF64 D, const double *pot, double *wtile,
+                             cudaStream_t st)
+{
+    if (ntiles_total <= 0) return cudaSuccess;
+    k_wtile_out<<<ntiles_total, 256, 0, st>>>(sets, tile_set, itile, ilist, D, pot, wtile);
     ++g_launches;
     return cudaGetLastError();
 }

@@ -1,0 +1,170 @@
+// sg_refine.cu -- FP64 recomputation of the rows whose split-FP32 sums may
+// miss the 1e-6 accuracy target.
+//
+// The split-FP32 kernel accumulates, per row, G^2 = sum over its j-tiles of
+// |FP32 tile sum|^2.  The FP32 rounding of the tile sums (the dominant error
+// term: the sub-block sums add into a 256-source tile sum in FP32) and of the
+// terms behaves like a random walk of size ~1e-7 G, so a row whose
+// acceleration cancels (|a| a few % of its G) can reach a relative error of
+// several 1e-6 even though its absolute error is ordinary.  The kernel also
+// marks (G = infinity) the rows lying more than 8 H from their i-tile centre,
+// whose FP32 tile-relative coordinate is rounded by enough to shift the row
+// measurably.  k_merge lists the rows with G > T |a| per set; this file
+// plans, on the device, an FP64 pass
+// over exactly those rows (k_fp64 over a device-written work list, so the
+// call needs no host round trip and stays graph-capturable) and scatters its
+// results over the FP32 ones.
+//
+// Determinism: the list order within a set depends on the merge's atomics,
+// but a row's FP64 sum depends only on its own pairs and on the chunk bounds,
+// which depend on the per-set counts alone; chunk sums merge in chunk order.
+#include "sg_launch.h"
+
+namespace sg {
+
+constexpr int PLAN_NT = 1024;
+
+// Exclusive block scan of one long long per thread (Hillis-Steele in shared
+// memory); returns the thread's prefix and writes the total to *total.
+__device__ long long block_exclusive_scan(long long v, long long *total)
+{
+    __shared__ long long s[PLAN_NT];
+    const int t = threadIdx.x;
+    s[t] = v;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+        const long long add = t >= o ? s[t - o] : 0;
+        __syncthreads();
+        s[t] += add;
+        __syncthreads();
+    }
+    const long long incl = s[t];
+    *total = s[blockDim.x - 1];
+    __syncthreads();
+    return incl - v;
+}
+
+// Sources per refine chunk: at least REFINE_MIN_J, so a few listed rows still
+// spread over many blocks (a listed row can have most of its set within its
+// softening length, e.g. a point-mass core, and pay the near-pair path for
+// most sources).
+constexpr int REFINE_MIN_J = 1024;
+
+__device__ __forceinline__ int refine_chunks(const SetDesc &S, int tj, int nch_global)
+{
+    const int jtiles = (S.n + tj - 1) / tj;
+    const int by_len = max(1, (int)(((long long)jtiles * tj) / REFINE_MIN_J));
+    return max(1, min(nch_global, min(by_len, max(1, jtiles))));
+}
+
+__global__ void __launch_bounds__(PLAN_NT) k_refine_plan(const SetDesc *sets, int nsets,
+                                                          const int *rcount, int itile, int tj,
+                                                          int target, int max_items,
+                                                          SetDesc *rsets, WorkItem *items,
+                                                          int *nitems, int *err)
+{
+    const int t = threadIdx.x;
+    const int per = (nsets + blockDim.x - 1) / blockDim.x;
+    const int s0 = min(nsets, t * per), s1 = min(nsets, s0 + per);
+    // pass 1: refine tiles of this thread's sets
+    long long tiles = 0;
+    for (int s = s0; s < s1; s++) {
+        const int r = min(rcount[s], sets[s].ni);
+        tiles += (r + itile - 1) / itile;
+    }
+    long long total_tiles = 0;
+    block_exclusive_scan(tiles, &total_tiles);
+    const int nch_global = total_tiles > 0 ? (int)max(1ll, (long long)target / total_tiles) : 1;
+    // pass 2: items of this thread's sets
+    long long cnt = 0;
+    for (int s = s0; s < s1; s++) {
+        const int r = min(rcount[s], sets[s].ni);
+        cnt += (long long)((r + itile - 1) / itile) * refine_chunks(sets[s], tj, nch_global);
+    }
+    long long total_items = 0;
+    long long base = block_exclusive_scan(cnt, &total_items);
+    if (total_items > max_items) {
+        if (t == 0) {
+            atomicOr(err, DEVERR_INPUT);
+            *nitems = 0;
+        }
+        return;
+    }
+    for (int s = s0; s < s1; s++) {
+        SetDesc S = sets[s];
+        const int r = min(rcount[s], S.ni);
+        const int nt = (r + itile - 1) / itile;
+        const int nch = refine_chunks(S, tj, nch_global);
+        const int jtiles = (S.n + tj - 1) / tj;
+        S.ni = r;
+        S.ntiles = nt;
+        S.nchunks = nch;
+        S.slot_off = (int)base;
+        rsets[s] = S;
+        for (int it = 0; it < nt; it++)
+            for (int c = 0; c < nch; c++) {
+                WorkItem w;
+                w.set = s;
+                w.tile = it;
+                w.chunk = c;
+                w.jb = (int)((long long)jtiles * c / nch) * tj;
+                w.je = (int)((long long)jtiles * (c + 1) / nch) * tj;
+                w.pad_[0] = w.pad_[1] = w.pad_[2] = 0;
+                items[base + (long long)it * nch + c] = w;
+            }
+        base += (long long)nt * nch;
+    }
+    if (t == 0) *nitems = (int)total_items;
+}
+
+cudaError_t launch_refine_plan(const SetDesc *sets, int nsets, const int *rcount, int itile,
+                               int tj, int target, int max_items, SetDesc *rsets,
+                               WorkItem *items, int *nitems, int *err, cudaStream_t st)
+{
+    k_refine_plan<<<1, PLAN_NT, 0, st>>>(sets, nsets, rcount, itile, tj, target, max_items, rsets,
+                                         items, nitems, err);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+__global__ void k_refine_merge(const SetDesc *sets, const SetDesc *rsets, const int *tile_set,
+                               int itile_main, int itile_ref, const int *rcount, const int *rlist,
+                               SortedF64 D, const double *rpart, OutputsDev out)
+{
+    const int t = blockIdx.x;
+    const int set = tile_set[t];
+    const SetDesc S = sets[set];
+    const int r = min(rcount[set], S.ni);
+    const int lt = t - S.tile_off;
+    const int l0 = lt * itile_main, l1 = min(r, l0 + itile_main);
+    if (l0 >= l1) return;
+    const SetDesc RS = rsets[set];
+    for (int li = l0 + threadIdx.x; li < l1; li += blockDim.x) {
+        const int rt = li / itile_ref, ri = li - rt * itile_ref;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int c = 0; c < RS.nchunks; c++) {
+            const double *p = rpart + (size_t)(RS.slot_off + rt * RS.nchunks + c) * 4 * itile_ref;
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] += p[q * itile_ref + ri];
+        }
+        const int o = D.orig[rlist[S.ioff + li]];
+        out.ax[o] = acc[0];
+        out.ay[o] = acc[1];
+        out.az[o] = acc[2];
+        out.pot[o] = acc[3];
+    }
+}
+
+cudaError_t launch_refine_merge(const SetDesc *sets, const SetDesc *rsets, const int *tile_set,
+                                int ntiles_main, int itile_main, int itile_ref, const int *rcount,
+                                const int *rlist, const SortedF64 D, const double *rpart,
+                                OutputsDev out, cudaStream_t st)
+{
+    if (ntiles_main <= 0) return cudaSuccess;
+    k_refine_merge<<<ntiles_main, 128, 0, st>>>(sets, rsets, tile_set, itile_main, itile_ref,
+                                                rcount, rlist, D, rpart, out);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+}  // namespace sg

@@ -2,8 +2,9 @@
 // alternative that the reference ships as a drop-in library with the same
 // C-ABI (misc/SPHgravtree_lib: grav_force_tree.cu over libSequoia), written
 // here from its semantics:
-//   * an octree over the Morton-sorted particles; a node splits while it
-//     holds more than TREE_LEAF particles (the reference: 64);
+//   * an octree over the Hilbert-sorted particles (an octree cell is a
+//     contiguous key range); a node splits while it holds more than
+//     TREE_LEAF particles (the reference: 64);
 //   * every node carries its mass, centre of mass and second moment about
 //     it (monopole + quadrupole, as libSequoia's body_node), built bottom-up
 //     in FP64; the walk uses the traceless quadrupole 3S - tr(S)I;
@@ -54,7 +55,7 @@ __device__ __forceinline__ int lower_bound_key(const unsigned long long *keys, i
 }
 
 // Children of node i of level `level` (keys of its particles share their
-// top 3*level Morton bits): the eight 3-bit digits of level + 1 split its
+// top 3*level key bits): the eight 3-bit digits of level + 1 split its
 // sorted range; b[0..8] are the digit boundaries.
 __device__ __forceinline__ void child_bounds(const TreeNode &T, int level,
                                              const unsigned long long *keys, int b[9])
@@ -119,7 +120,7 @@ __device__ void emit_children(int i, int l0, int level, int next_base, TreeNode 
     T.nchild = c;
     nodes[i] = T;
     // Children of a node too big to be a group become groups, consecutive
-    // small siblings merged (Morton order) while they total <= TREE_GROUP:
+    // small siblings merged (curve order) while they total <= TREE_GROUP:
     // gflag of a run's first child = the run's length in nodes.
     const bool big = T.end - T.start > TREE_GROUP;
     int run = -1, run_len = 0, run_n = 0;

@@ -103,28 +103,41 @@ def forces_row_split(compute: RowCompute, x, y, z, m, range2, group=None):
 
 
 def forces_set_shard(compute: RowCompute, offsets, x, y, z, m, range2, group=None):
-    """Batches: whole sets per rank (LPT by N^2), all results gathered."""
+    """Batches: whole sets per rank (LPT by N^2), all results gathered.  Each
+    rank packs the rows of its own sets, in set order, into a (4, k) block;
+    the blocks are all-gathered (padded to the largest) and unpacked with the
+    set assignment every rank knows, so no rank sends rows it does not own."""
     import torch
     import torch.distributed as dist
     nranks = dist.get_world_size(group)
     rank = dist.get_rank(group)
     offsets = np.asarray(offsets)
     sizes = np.diff(offsets)
-    mine = shard_sets(sizes, nranks)[rank]
+    shards = shard_sets(sizes, nranks)
     n = int(offsets[-1])
-    local = np.zeros((4, n))
-    owned = np.zeros(n)
-    for s in mine:
+    counts = [int(sum(int(sizes[s]) for s in shards[r])) for r in range(nranks)]
+    width = max(1, max(counts))
+    block = np.zeros((4, width))
+    col = 0
+    for s in shards[rank]:
         a, b = int(offsets[s]), int(offsets[s + 1])
         res = compute(x[a:b], y[a:b], z[a:b], m[a:b], range2[a:b], 0, b - a)
         for q in range(4):
-            local[q, a:b] = np.asarray(res[q])[: b - a]
-        owned[a:b] = 1.0
-    t = torch.from_numpy(np.vstack([local, owned[None, :]])).to(comm_device(group))
-    dist.all_reduce(t, group=group)  # each row is owned by exactly one rank
-    t = t.cpu().numpy()
-    assert np.all(t[4] == 1.0)
-    return tuple(t[q].copy() for q in range(4))
+            block[q, col:col + b - a] = np.asarray(res[q])[: b - a]
+        col += b - a
+    dev = comm_device(group)
+    t = torch.from_numpy(block).to(dev)
+    bufs = [torch.empty_like(t) for _ in range(nranks)]
+    dist.all_gather(bufs, t, group=group)
+    out = np.zeros((4, n))
+    for r in range(nranks):
+        got = bufs[r].cpu().numpy()
+        col = 0
+        for s in shards[r]:
+            a, b = int(offsets[s]), int(offsets[s + 1])
+            out[:, a:b] = got[:, col:col + b - a]
+            col += b - a
+    return tuple(out[q].copy() for q in range(4))
 
 
 def gpu_compute(ctx, nkernel: int = 0, precision: str = "f32split") -> RowCompute:
@@ -158,17 +171,16 @@ def forces_row_split_device(compute: DeviceRowCompute, own, n: int, group=None):
 
 
 def gpu_compute_device(ctx, nkernel: int = 0, precision: str = "f32split") -> DeviceRowCompute:
-    """Per-rank computation with the GPU library on device tensors.  The
-    library runs on the context's stream: torch's stream (where the gathered
-    sources and the zeroed outputs were written) is drained first, and the
-    call returns after the library finished, so the collective that follows
-    sees the rows."""
+    """Per-rank computation with the GPU library on device tensors, stream
+    ordered: the library is pointed at torch's current stream, where the
+    gathered sources and the zeroed outputs were written and where the
+    collective that follows is enqueued, so no host synchronisation is
+    needed between the all-gathers and the gravity call."""
     import torch
 
     def f(src, i_begin, ni, out):
-        torch.cuda.current_stream(src.device).synchronize()
+        ctx.set_stream(torch.cuda.current_stream(src.device).cuda_stream)
         n = src.shape[1]
         ctx.forces_device(n, src[0], src[1], src[2], src[3], src[4], out[0], out[1], out[2],
                           out[3], nkernel=nkernel, precision=precision, i_begin=i_begin, ni=ni)
-        ctx.sync()
     return f

@@ -63,7 +63,8 @@ def read_snapshot(path: str) -> Snapshot:
         off += 4
         if n2 != n:
             raise ValueError(f"{path}: corrupt record framing at byte {off}")
-    ntot = struct.unpack_from("<i", buf, recs[0][0])[0]
+    if len(recs) < 2:
+        raise ValueError(f"{path}: {len(recs)} records; a dump has a header and a trailer")
     header, nhf = {}, 0
     for nf in (HEADER_FULL, HEADER_OLD):
         if struct.calcsize(_header_format(nf)) == recs[0][1]:
@@ -71,14 +72,24 @@ def read_snapshot(path: str) -> Snapshot:
             header = {name: v for (name, _), v in zip(HEADER[:nf], vals)}
             nhf = nf
             break
+    if not nhf:
+        raise ValueError(f"{path}: unexpected header length {recs[0][1]}")
+    ntot = int(header["ntot"])
     body = recs[1:-1]
     if len(body) != ntot:
         raise ValueError(f"{path}: header says {ntot} particles, found {len(body)} records")
+    if recs[-1][1] != 4:
+        raise ValueError(f"{path}: trailing record of {recs[-1][1]} bytes, expected 4")
     tail = struct.unpack_from("<i", buf, recs[-1][0])[0]
     if tail != ntot:
         raise ValueError(f"{path}: trailing ntot {tail} != {ntot}")
+    if ntot == 0:
+        data = {name: np.zeros(0) for name in FIELDS}
+        data["cc"] = np.zeros(0, dtype=np.int32)
+        data["divv"] = np.zeros(0)
+        return Snapshot(0, data, header, nhf)
     reclen = body[0][1]
-    if reclen not in (140, 156):
+    if reclen not in (140, 156) or any(r[1] != reclen for r in body):
         raise ValueError(f"{path}: unexpected particle record length {reclen}")
     start = body[0][0]
     stride = reclen + 8
@@ -92,8 +103,6 @@ def read_snapshot(path: str) -> Snapshot:
         extra = np.ascontiguousarray(raw[:, 140:156]).view("<f8").reshape(ntot, 2)
         data["ueq"] = extra[:, 0].copy()
         data["tthermal"] = extra[:, 1].copy()
-    if not nhf:
-        raise ValueError(f"{path}: unexpected header length {recs[0][1]}")
     return Snapshot(ntot, data, header, nhf)
 
 

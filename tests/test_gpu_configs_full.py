@@ -1,0 +1,200 @@
+"""Full-size parity of the benchmark workloads (configs 2-5) against the oracle,
+the C restatement of the reference's CPU path (parallel_bleeding_edge/src/
+cpu_grav.f:1-381: far field :59-70, near field :71-157, zero distance
+:138-145).
+
+Per particle relative errors of the acceleration |a - a_ref| / |a_ref| and
+of the potential; particles with |a| < 1e-3 median |a| are excluded from the
+acceleration maximum (cancellation makes their relative error
+ill-conditioned), as everywhere in these tests.  Tolerances:
+  FP64 kernel     <= 1e-12 against the oracle
+  split-FP32      <= 1e-6  against the oracle, and against the FP64 kernel on
+                           every row (the FP64 kernel being pinned to the
+                           oracle on the sampled rows)
+
+Rows checked against the oracle: every row of config 2 (the faithful
+triangle); for configs 3-5 a seeded sample per set plus the rows most likely
+to fail -- the smallest |a| (cancellation) and, for config 3, the point-mass
+core (row 0).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import err_report
+from starsmasher_b200 import Context, inputs
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+F32_TOL = 1e-6
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dev(a):
+    return _torch().as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def _run(ctx, ws, X, precision):
+    t = _torch()
+    outs = [t.empty(ws.n, dtype=t.float64, device="cuda") for _ in range(4)]
+    if ws.nsets > 1:
+        ctx.batch_forces_device(ws.offsets, *X, *outs, nkernel=0, precision=precision)
+    else:
+        ctx.forces_device(ws.n, *X, *outs, nkernel=0, precision=precision)
+    ctx.sync()
+    return [o.cpu().numpy() for o in outs]
+
+
+def _amag(r):
+    return np.sqrt(r[0] ** 2 + r[1] ** 2 + r[2] ** 2)
+
+
+def _rows_for_set(a, b, amag, rng, nrand, nsmall):
+    """Seeded random rows of set [a, b) plus its nsmall smallest-|a| rows."""
+    n = b - a
+    pick = rng.choice(n, min(n, nrand), replace=False)
+    small = np.argsort(amag[a:b])[:nsmall]
+    return a + np.unique(np.concatenate([pick, small]))
+
+
+def _oracle_on_rows(ws, rows):
+    """oracle.rows for global row indices (any sets): (ax, ay, az, pot)."""
+    out = [np.zeros(len(rows)) for _ in range(4)]
+    setid = np.searchsorted(ws.offsets, rows, side="right") - 1
+    for s in np.unique(setid):
+        a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
+        k = np.nonzero(setid == s)[0]
+        r = oracle.rows(ws.x[a:b], ws.y[a:b], ws.z[a:b], ws.m[a:b], ws.range2[a:b], 0,
+                        row_idx=(rows[k] - a).astype(np.int32))
+        for q in range(4):
+            out[q][k] = r[q]
+    return out
+
+
+def _check_rows(got, ref, rows, median_a, tol, what):
+    """Relative errors on `rows` with the workload's median |a| as the
+    ill-conditioning reference."""
+    g = [np.asarray(x)[rows] for x in got]
+    amag = _amag(ref)
+    e = np.sqrt(sum((g[q] - ref[q]) ** 2 for q in range(3))) / amag
+    ok = amag >= 1e-3 * median_a
+    ep = np.abs(g[3] - ref[3]) / np.abs(ref[3])
+    acc_max = float(e[ok].max()) if ok.any() else 0.0
+    print(what, f"rows={len(rows)} acc_max={acc_max:.3e} pot_max={ep.max():.3e}")
+    assert acc_max <= tol, (what, acc_max)
+    assert ep.max() <= tol, (what, float(ep.max()))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    t = _torch()
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def test_config2_every_row_against_the_cpu_path(ctx):
+    """Two-star collision, N = 262,144: every row against the faithful
+    triangle (cpu_grav.f's j >= i loop with Newton's third law)."""
+    ws = inputs.cached("config2")
+    X = [_dev(a) for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
+    tri = oracle.triangle(ws.x, ws.y, ws.z, ws.m, ws.range2, 0)
+    for precision, tol in (("fp64", FP64_TOL), ("f32split", F32_TOL)):
+        got = _run(ctx, ws, X, precision)
+        r = err_report(*got, *tri)
+        print("config2", precision, r)
+        assert r["acc_max"] <= tol and r["pot_max"] <= tol, (precision, r)
+        if precision == "fp64":
+            assert r["acc_max_ill"] <= 1e-9, r
+
+
+def test_config3_sampled_rows_and_core(ctx):
+    """Red giant with a point-mass core, N = 1,048,576: 4,096 seeded rows,
+    the 64 smallest |a| and the core (row 0) against the oracle; split-FP32
+    against the FP64 kernel on every row."""
+    ws = inputs.cached("config3")
+    X = [_dev(a) for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
+    r64 = _run(ctx, ws, X, "fp64")
+    r32 = _run(ctx, ws, X, "f32split")
+    amag = _amag(r64)
+    med = float(np.median(amag))
+    rng = np.random.default_rng(33)
+    rows = np.unique(np.concatenate([[0], _rows_for_set(0, ws.n, amag, rng, 4096, 64)]))
+    ref = _oracle_on_rows(ws, rows)
+    _check_rows(r64, ref, rows, med, FP64_TOL, "config3 fp64 vs oracle")
+    _check_rows(r32, ref, rows, med, F32_TOL, "config3 f32split vs oracle")
+    r = err_report(*r32, *r64)
+    print("config3 f32split vs fp64, all rows", r)
+    assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
+
+
+def test_config4_all_64_models(ctx):
+    """64 uneven models in one batched launch: per model 128 seeded rows and
+    its 8 smallest |a| against the oracle; split-FP32 against the FP64
+    kernel on every row of every model."""
+    ws = inputs.cached("config4")
+    assert ws.nsets == 64
+    X = [_dev(a) for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
+    r64 = _run(ctx, ws, X, "fp64")
+    r32 = _run(ctx, ws, X, "f32split")
+    amag = _amag(r64)
+    med = float(np.median(amag))
+    rng = np.random.default_rng(44)
+    rows = np.concatenate([_rows_for_set(int(ws.offsets[s]), int(ws.offsets[s + 1]), amag, rng,
+                                         128, 8) for s in range(ws.nsets)])
+    ref = _oracle_on_rows(ws, rows)
+    _check_rows(r64, ref, rows, med, FP64_TOL, "config4 fp64 vs oracle")
+    _check_rows(r32, ref, rows, med, F32_TOL, "config4 f32split vs oracle")
+    r = err_report(*r32, *r64)
+    print("config4 f32split vs fp64, all rows", r)
+    assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
+
+
+def test_config5_graph_sweep_first_and_last_call(ctx):
+    """16 collision snapshots swept by a captured graph (seeded kick of 1e-3
+    R, then gravity): call 1 and call 203.  The kicks between them do not
+    depend on gravity, so calls 2-202 are replayed as kicks only.  At both
+    calls: 64 seeded rows and the 8 smallest |a| per snapshot against the
+    oracle on the kicked positions, split-FP32 against the FP64 kernel on
+    every row."""
+    t = _torch()
+    ws = inputs.cached("config5")
+    X = [_dev(a) for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
+    outs = [t.empty(ws.n, dtype=t.float64, device="cuda") for _ in range(4)]
+    rng = np.random.default_rng(55)
+    with Context(0) as g:
+        g.batch_forces_device(ws.offsets, *X, *outs, nkernel=0, precision="f32split")
+        g.sync()
+        g.kick_reset(0)
+        with g.capture() as cap:
+            g.kick_device(ws.n, X[0], X[1], X[2], 1e-3, 12345)
+            g.batch_forces_device(ws.offsets, *X, *outs, nkernel=0, precision="f32split")
+        graph = cap.graph
+        for call in (1, 203):
+            if call > 1:
+                for _ in range(call - 2):
+                    g.kick_device(ws.n, X[0], X[1], X[2], 1e-3, 12345)
+            graph.launch(1)
+            g.sync()
+            r32 = [o.cpu().numpy() for o in outs]
+            r64 = _run(ctx, ws, X, "fp64")
+            amag = _amag(r64)
+            med = float(np.median(amag))
+            pos = [x.cpu().numpy() for x in X]
+            kicked = inputs.ParticleSets(pos[0], pos[1], pos[2], pos[3], pos[4], ws.offsets)
+            rows = np.concatenate([_rows_for_set(int(ws.offsets[s]), int(ws.offsets[s + 1]), amag,
+                                                 rng, 64, 8) for s in range(ws.nsets)])
+            ref = _oracle_on_rows(kicked, rows)
+            _check_rows(r64, ref, rows, med, FP64_TOL, f"config5 call {call} fp64 vs oracle")
+            _check_rows(r32, ref, rows, med, F32_TOL, f"config5 call {call} f32split vs oracle")
+            r = err_report(*r32, *r64)
+            print(f"config5 call {call} f32split vs fp64, all rows", r)
+            assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
+        graph.close()

@@ -302,21 +302,65 @@ def test_red_giant_core_subset(gpu_ctx):
     assert r64["acc_max"] <= FP64_TOL and r64["pot_max"] <= FP64_TOL, r64
 
 
-@pytest.mark.parametrize("band", [1.0, 1.5, 3.0])
+@pytest.mark.parametrize("band", [1.0, 1.5, 2.0, 3.0])
 def test_fp64_band_setting(gpu_ctx, star16k, tri16k, band):
     """sphgrav_set_fp64_band moves pairs between two correct evaluations: every
-    setting stays accurate (band 1 keeps only the softened near field in FP64,
-    so its worst, cancellation-dominated particle may exceed 1e-6)."""
+    setting stays within 1e-6 (band 1, the default, keeps only the softened
+    near field in FP64; the refine recomputes the rows whose FP32 sums are
+    ill-conditioned)."""
     s = star16k
     try:
         gpu_ctx.set_fp64_band(band)
         got = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
     finally:
-        gpu_ctx.set_fp64_band(2.0)
+        gpu_ctx.set_fp64_band(1.0)
     r = err_report(*got, *tri16k[0])
     print("band", band, r)
     assert r["acc_rms"] <= 1e-7 and r["pot_max"] <= F32_TOL
-    assert r["acc_max"] <= (3 * F32_TOL if band < 2.0 else F32_TOL), r
+    assert r["acc_max"] <= F32_TOL, r
+
+
+def test_refine_recomputes_listed_rows_in_fp64(gpu_ctx):
+    """The FP64 refine: with the refine off the split-FP32 sums stand for
+    every row; with it on, exactly the rows whose error scale G exceeds
+    |a| (or that lie far from their tile centre, G = inf) change, and
+    those rows then agree with the CPU path to the FP64 tolerance; the
+    others are bit-identical."""
+    s = inputs.collision_snapshots(1, 24000, 24000, seed=8)
+    try:
+        gpu_ctx.keep_error_scale(True)
+        gpu_ctx.set_refine(0.0)
+        off = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
+        assert gpu_ctx.last_refine_rows() == 0
+        G = gpu_ctx.error_scale(s.n)
+        gpu_ctx.set_refine(1.0)
+        on = gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
+        nref = gpu_ctx.last_refine_rows()
+    finally:
+        gpu_ctx.keep_error_scale(False)
+        gpu_ctx.set_refine(1.0)
+    amag = np.sqrt(off[0] ** 2 + off[1] ** 2 + off[2] ** 2)
+    listed = G > amag
+    assert nref == int(listed.sum()) and nref > 0
+    same = np.all([np.equal(a, b) for a, b in zip(on, off)], axis=0)
+    assert np.all(same[~listed])
+    rows = np.nonzero(listed)[0].astype(np.int32)
+    o = oracle.rows(s.x, s.y, s.z, s.m, s.range2, 0, row_idx=rows)
+    r = err_report(*(a[rows] for a in on), *o)
+    print("refined rows", nref, r)
+    assert r["acc_max"] <= FP64_TOL and r["pot_max"] <= FP64_TOL, r
+
+
+def test_error_scale_needs_keep(gpu_ctx, star16k):
+    s = star16k
+    gpu_ctx.keep_error_scale(False)
+    gpu_ctx.forces(s.x, s.y, s.z, s.m, s.range2, 0, "f32split")
+    with pytest.raises(_lib.SphgravError) as e:
+        gpu_ctx.error_scale(s.n)
+    assert e.value.status == _lib.ERR_PROTOCOL
+    for bad in (-0.5, float("nan"), 1e7):
+        with pytest.raises(_lib.SphgravError):
+            gpu_ctx.set_refine(bad)
 
 
 def test_fp64_band_rejects_bad_values(gpu_ctx):

@@ -1,5 +1,6 @@
 """CPU tests of the workload generators and the snapshot reader and writer."""
 import os
+import struct
 
 import numpy as np
 import pytest
@@ -132,3 +133,22 @@ def test_snapshots_as_a_batch(tmp_path):
         np.testing.assert_array_equal(b.m[a:e], d["am"])
         want = np.where(d["u"] == 0.0, -4.0 * d["hp"] ** 2, 4.0 * d["hp"] ** 2)
         np.testing.assert_array_equal(b.range2[a:e], want)
+
+
+def test_snapshot_empty_roundtrip(tmp_path):
+    """A dump with ntot = 0 (which the writer produces) reads back as an empty
+    snapshot; a file with a bad header length is rejected before its body is
+    parsed."""
+    from starsmasher_b200.snapshot import FIELDS
+    path = str(tmp_path / "empty.sph")
+    write_snapshot(path, Snapshot(0, {}, {"t": 1.5}))
+    back = read_snapshot(path)
+    assert back.ntot == 0 and back.header["t"] == 1.5
+    for k in FIELDS:
+        assert back.data[k].shape == (0,)
+    bad = str(tmp_path / "bad.sph")
+    with open(bad, "wb") as f:
+        f.write(struct.pack("<i", 12) + b"\0" * 12 + struct.pack("<i", 12))
+        f.write(struct.pack("<iii", 4, 0, 4))
+    with pytest.raises(ValueError, match="header length"):
+        read_snapshot(bad)

@@ -44,10 +44,15 @@ def _rel(a, b):
     return float((da / amag)[ok].max()), float((np.abs(pot - bp) / np.abs(bp)).max())
 
 
-@pytest.mark.parametrize("nkernel,n,seed", [(0, 6000, 71), (2, 1537, 72)])
+# The last case fills the scratch exactly: at SPHGRAV_NOALLOC_MAX_N one chunk's
+# 4 n partial sums are the whole static array.
+@pytest.mark.parametrize("nkernel,n,seed", [(0, 6000, 71), (1, 4099, 73), (2, 1537, 72),
+                                            (1, "max", 74)])
 def test_noalloc_matches_forces_device_twice(gpu_ctx, nkernel, n, seed):
     import torch
     lib = _lib.load()
+    if n == "max":
+        n = _noalloc_max_n()
     s = inputs.single_polytrope(n, 1.5, seed=seed)
     s.range2[::97] *= -1.0  # some point masses
     X = [_dev(a) for a in (s.x, s.y, s.z, s.m, s.range2)]
