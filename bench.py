@@ -384,7 +384,7 @@ def main():
 
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     device = local if world > 1 else 0
     torch.cuda.set_device(device)
@@ -428,13 +428,12 @@ def main():
         # the reference's gravity row split: this rank owns rows [lo, hi)
         lo, hi = multirank.gpu_row_range(n, world, rank)
         own = torch.stack([t[lo:hi] for t in X]).contiguous()
-        compute = {p: multirank.gpu_compute_device(ctx, args.nkernel, p) for p in ("f32split", "fp64")}
+        split = {p: multirank.RowSplitStep(multirank.gpu_compute_device(ctx, args.nkernel, p), own, n)
+                 for p in ("f32split", "fp64")}
         mode = f"row split x{world} (main.f:283-295): NCCL all-gather of sources and rows"
-        split_out = {}
 
         def step(precision):
-            src, res = multirank.forces_row_split_device(compute[precision], own, n)
-            split_out["res"] = res
+            split[precision]()
     else:
         shards = multirank.shard_sets(np.diff(ws.offsets), world)[rank]
         sub = [(int(ws.offsets[s]), int(ws.offsets[s + 1])) for s in shards]
@@ -625,7 +624,7 @@ def main():
 
             def e2e_step():
                 own_d = own_h.to(f"cuda:{device}", non_blocking=True)
-                src, res = multirank.forces_row_split_device(compute[args.precision], own_d, n)
+                src, res = split[args.precision](own_d)
                 res_h.copy_(res, non_blocking=True)
                 torch.cuda.current_stream().synchronize()
             how = "row split from host arrays (pinned H2D of own rows, D2H of all rows)"

@@ -103,7 +103,8 @@ int sphgrav_legacy_set_precision(int precision);
 int sphgrav_create(sphgrav_ctx **ctx, int device);
 int sphgrav_destroy(sphgrav_ctx *ctx);
 /* Use an existing cudaStream_t (passed as void*) instead of the context's
- * own stream; NULL restores the context's stream. */
+ * own stream; NULL restores the context's stream (pass cudaStreamLegacy,
+ * (void *)1, for the legacy default stream). */
 int sphgrav_set_stream(sphgrav_ctx *ctx, void *stream);
 /* Wait for all work queued on the context and report a device-side error
  * (invalid input found on the device, timeout) recorded since the last call. */

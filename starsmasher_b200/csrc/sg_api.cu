@@ -311,10 +311,11 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
         int v = variant_by_name(precision, it->second);
         if (v >= 0) return v;
     }
-    // FP64: two rows per thread from 2^18 on (config 2: 810 vs 754 G pairs/s,
-    // config 3: 883 vs 826), one row below (16K: 276 vs 194; the batch of
-    // 4K-131K models: 735 vs 727)
-    if (precision == SPHGRAV_FP64) return b >= 18 ? 1 : 0;
+    // FP64: two rows per thread and 256-source tiles from 2^18 on (262K:
+    // 804 vs 769 G pairs/s for one row per thread; 1M: 892 vs 831), one row
+    // and 128-source tiles below (16K: 224 vs 162; the batch of 4K-131K
+    // models: 725 vs 694)
+    if (precision == SPHGRAV_FP64) return b >= 18 ? 4 : 0;
     // defaults by pair-weighted mean N = 2^b, from a sweep of single
     // polytropes on B200 (G pairs/s of the chosen shape vs the runner-up):
     //   b >= 20  W12K2Q1, 7 stages   (1M: 2027 vs 1942 for W15K1Q2)

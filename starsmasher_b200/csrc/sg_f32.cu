@@ -37,9 +37,13 @@
 //     staged sources are re-expressed relative to the i-tile's centre c:
 //     x' = (x_hi - c_hi) + (x_lo - c_lo), a few flops per staged particle
 //     instead of per pair.
-//   * sums run in FP32 over sub-blocks (8 terms per accumulator lane), are
-//     added into a per-tile FP32 sum that folds into compensated (TwoSum,
-//     "Kahan") float hi/lo accumulators in shared memory once per tile.
+//   * acceleration sums run in FP32 over sub-blocks (8 terms per
+//     accumulator lane), are added into a per-tile FP32 sum that folds into
+//     compensated (TwoSum, "Kahan") float hi/lo accumulators in shared memory
+//     once per tile; the potential terms, all of one sign, go straight into
+//     the tile sum in the far loop.  Per row the kernel also keeps G^2, the
+//     sum over tiles of |FP32 tile sum|^2 (the scale of the FP32 rounding
+//     error), for the FP64 refine of ill-conditioned rows (sg_refine.cu).
 //   * pairs with r < 2 max(H_i, H_j) are masked out of the FP32 sums by the
 //     checked loop, flagged in per-thread bit masks, and evaluated after the
 //     tile's FP32 loop in FP64 with the CPU-path formulas, one pair per lane
@@ -204,7 +208,7 @@ __device__ __noinline__ void near_eval(const SortedF64 D, int nkernel, int jbase
                 const double xj = (double)rs[j] + (double)rs[TJ + j];
                 const double yj = (double)rs[2 * TJ + j] + (double)rs[3 * TJ + j];
                 const double zj = (double)rs[4 * TJ + j] + (double)rs[5 * TJ + j];
-                const PairOut o = pair_f64_core(D, nkernel, ipo, jbase + j, xj - row[0],
+                const PairOut o = pair_f64_fast(D, nkernel, ipo, jbase + j, xj - row[0],
                                                 yj - row[NT], zj - row[2 * NT], rd[j], row[3 * NT],
                                                 rd[TJ + j]);
                 res2[lane] = make_double2(o.ax, o.ay);
@@ -274,12 +278,15 @@ struct WsSmem {
 // the rows of the benchmark workloads lie beyond 8 H).
 constexpr float SHIFT_H = 8.f;
 
-template <int W, int K, int Q, int TJ, int NS, bool NEWTON>
+template <int W, int K, int Q, int TJ, int NS, bool NEWTON, int FQ>
 __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 {
     static_assert(32 % Q == 0, "threads per row must divide a warp");
-    constexpr int SUBQ = 4;                // quads per sub-block (8 sources per lane)
+    constexpr int SUBQ = 4;                // quads per checked-loop sub-block (8 sources per lane)
     static_assert((TJ / 4) % (Q * SUBQ) == 0, "j-tile must hold whole sub-blocks");
+    // far loop: FQ quads per sub-block (2 FQ sources per packed lane in one
+    // FP32 FMA chain before the sub-block sum is added to the tile sum)
+    static_assert((TJ / 4) % (Q * FQ) == 0, "j-tile must hold whole far sub-blocks");
     static_assert(TJ % 32 == 0, "producer lanes split the tile");
     using L = WsSmem<W, K, Q, TJ, NS>;
     constexpr int NT = L::NT;              // consumer threads
@@ -527,12 +534,15 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     uint32_t wsum = 0;  // non-empty near masks of this thread (bit k*NSB + sb)
 
                     if (far) {
-                        for (int base = phase; base < TJ / 4; base += Q * SUBQ) {
-                            f2 ax[K], ay[K], az[K], pp[K];
+                        // the potential terms are all positive (no cancellation), so
+                        // they go straight into the tile sum; the acceleration
+                        // components, which cancel, keep the sub-block sums
+                        for (int base = phase; base < TJ / 4; base += Q * FQ) {
+                            f2 ax[K], ay[K], az[K];
 #pragma unroll
-                            for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pp[k] = pk(0.f, 0.f);
+                            for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pk(0.f, 0.f);
 #pragma unroll  // whole sub-block: +5% at N=1M over unroll 2
-                            for (int u = 0; u < SUBQ; u++) {
+                            for (int u = 0; u < FQ; u++) {
                                 const int qd = base + u * Q;
                                 const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(&s_x[4 * qd]);
                                 const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(&s_y[4 * qd]);
@@ -542,9 +552,9 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                                 for (int k = 0; k < K; k++) {
                                     f2 dx, dy, dz, r2;
                                     geom2(X.x, Y.x, Z.x, xi[k], yi[k], zi[k], dx, dy, dz, r2);
-                                    accum2<NEWTON>(dx, dy, dz, r2, M.x, ax[k], ay[k], az[k], pp[k]);
+                                    accum2<NEWTON>(dx, dy, dz, r2, M.x, ax[k], ay[k], az[k], tp[k]);
                                     geom2(X.y, Y.y, Z.y, xi[k], yi[k], zi[k], dx, dy, dz, r2);
-                                    accum2<NEWTON>(dx, dy, dz, r2, M.y, ax[k], ay[k], az[k], pp[k]);
+                                    accum2<NEWTON>(dx, dy, dz, r2, M.y, ax[k], ay[k], az[k], tp[k]);
                                 }
                             }
 #pragma unroll
@@ -552,7 +562,6 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                                 tx[k] = add2(tx[k], ax[k]);
                                 ty[k] = add2(ty[k], ay[k]);
                                 tz[k] = add2(tz[k], az[k]);
-                                tp[k] = add2(tp[k], pp[k]);
                             }
                         }
                     } else {
@@ -679,25 +688,28 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     }
 }
 
-// name, consumer warps W, rows per thread K, threads per row Q, j-tile TJ, stages NS, Newton step
-#define SG_F32_VARIANTS(X)                                           \
-    X(12, 2, 1, 256, 7, false, "f32split_w12_k2_q1_tj256_ns7")        \
-    X(15, 2, 1, 256, 4, false, "f32split_w15_k2_q1_tj256")            \
-    X(12, 1, 1, 256, 7, false, "f32split_w12_k1_q1_tj256_ns7")        \
-    X(15, 1, 2, 256, 4, false, "f32split_w15_k1_q2_tj256")            \
-    X(8, 1, 4, 256, 4, false, "f32split_w8_k1_q4_tj256")              \
-    X(12, 1, 4, 256, 7, false, "f32split_w12_k1_q4_tj256_ns7")        \
-    X(15, 2, 1, 256, 4, true, "f32split_w15_k2_q1_tj256_newton")      \
-    X(15, 1, 2, 256, 4, true, "f32split_w15_k1_q2_tj256_newton")      \
-    X(8, 1, 4, 256, 4, true, "f32split_w8_k1_q4_tj256_newton")
+// name, consumer warps W, rows per thread K, threads per row Q, j-tile TJ,
+// stages NS, Newton step, quads per far-loop sub-block FQ
+#define SG_F32_VARIANTS(X)                                              \
+    X(12, 2, 1, 256, 7, false, 4, "f32split_w12_k2_q1_tj256_ns7")        \
+    X(15, 2, 1, 256, 4, false, 4, "f32split_w15_k2_q1_tj256")            \
+    X(12, 1, 1, 256, 7, false, 4, "f32split_w12_k1_q1_tj256_ns7")        \
+    X(15, 1, 2, 256, 4, false, 4, "f32split_w15_k1_q2_tj256")            \
+    X(8, 1, 4, 256, 4, false, 4, "f32split_w8_k1_q4_tj256")              \
+    X(12, 1, 4, 256, 7, false, 4, "f32split_w12_k1_q4_tj256_ns7")        \
+    X(15, 2, 1, 256, 4, true, 4, "f32split_w15_k2_q1_tj256_newton")      \
+    X(15, 1, 2, 256, 4, true, 4, "f32split_w15_k1_q2_tj256_newton")      \
+    X(8, 1, 4, 256, 4, true, 4, "f32split_w8_k1_q4_tj256_newton")        \
+    X(12, 2, 1, 256, 7, false, 8, "f32split_w12_k2_q1_tj256_ns7_fq8")    \
+    X(12, 1, 1, 256, 7, false, 8, "f32split_w12_k1_q1_tj256_ns7_fq8")
 
-#define SG_INFO(W, K, Q, TJ, NS, NW, NAME) {1, (W + 1) * 32, K, Q, TJ, NW ? 1 : 0, NAME, W * 32 * K / Q},
+#define SG_INFO(W, K, Q, TJ, NS, NW, FQ, NAME) {1, (W + 1) * 32, K, Q, TJ, NW ? 1 : 0, NAME, W * 32 * K / Q},
 static const VariantInfo kF32Variants[] = {SG_F32_VARIANTS(SG_INFO)};
 #undef SG_INFO
-#define SG_PTR(W, K, Q, TJ, NS, NW, NAME) (const void *)k_f32split<W, K, Q, TJ, NS, NW>,
+#define SG_PTR(W, K, Q, TJ, NS, NW, FQ, NAME) (const void *)k_f32split<W, K, Q, TJ, NS, NW, FQ>,
 static const void *kF32Kernels[] = {SG_F32_VARIANTS(SG_PTR)};
 #undef SG_PTR
-#define SG_SMEM(W, K, Q, TJ, NS, NW, NAME) WsSmem<W, K, Q, TJ, NS>::BYTES,
+#define SG_SMEM(W, K, Q, TJ, NS, NW, FQ, NAME) WsSmem<W, K, Q, TJ, NS>::BYTES,
 static const int kF32Smem[] = {SG_F32_VARIANTS(SG_SMEM)};
 #undef SG_SMEM
 constexpr int kNF32 = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
@@ -724,9 +736,9 @@ cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st)
     cudaError_t e = f32_prepare(v);
     if (e != cudaSuccess) return e;
     int idx = 0;
-#define SG_CASE(W, K, Q, TJ, NS, NW, NAME)                                                    \
+#define SG_CASE(W, K, Q, TJ, NS, NW, FQ, NAME)                                                \
     if (v == idx) {                                                                           \
-        k_f32split<W, K, Q, TJ, NS, NW><<<grid, (W + 1) * 32, WsSmem<W, K, Q, TJ, NS>::BYTES, st>>>(a); \
+        k_f32split<W, K, Q, TJ, NS, NW, FQ><<<grid, (W + 1) * 32, WsSmem<W, K, Q, TJ, NS>::BYTES, st>>>(a); \
         ++g_launches;                                                                         \
         return cudaGetLastError();                                                            \
     }                                                                                         \

@@ -14,8 +14,9 @@
 //   * per (warp, tile) a box test: when every pair of the warp's rows with
 //     the tile's sources is Newtonian (r^2 > max H^2 for all of them), the
 //     tile runs a loop without the per-pair branch;
-//   * one FP64 partial sum per (row, j-chunk), merged in chunk order by
-//     k_merge.
+//   * per row, each j-tile's plain FP64 sums fold into TwoSum-compensated
+//     running sums; one FP64 partial sum per (row, j-chunk), merged in chunk
+//     order by k_merge.
 // Far pairs take 1/r from the PTX rsqrt.approx.ftz.f64 seed y0 refined by one
 // third-order step of the series (1 - e)^(-1/2) = 1 + e/2 + 3e^2/8 + O(e^3),
 // e = 1 - r^2 y0^2 (Householder's method for x^(-1/2)): 5 FP64 operations
@@ -40,8 +41,15 @@ __device__ __forceinline__ double rsqrt_f64(double r2)
     return fma(y0, q, y0);
 }
 
+// Resident blocks per SM the register budget is sized for: 64K registers /
+// (NT * MINB) per thread (K = 1: 128, K = 2: 170, K = 4: 255 at NT = 128).
+template <int NT, int K>
+struct F64Occ {
+    static constexpr int MINB = (K >= 4 ? 2 : (K == 2 ? 3 : 4)) * 128 / NT;
+};
+
 template <int NT, int K, int TJ, int NS>
-__global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
+__global__ void __launch_bounds__(NT, F64Occ<NT, K>::MINB) k_fp64(ComputeArgs a)
 {
     static_assert(TJ % META_J == 0, "j-tile must hold whole metadata records");
     constexpr int ITILE = NT * K;
@@ -51,6 +59,7 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
     __shared__ __align__(128) double s_src[NS][5][TJ];  // x y z m H^2
     __shared__ __align__(16) JMeta s_meta[NS][NMETA];
     __shared__ __align__(8) uint64_t s_bar[NS];
+    __shared__ double s_lo[4][K][NT];  // low parts of the compensated running sums
     __shared__ int s_item;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const SortedF64 D = a.D;
@@ -98,7 +107,8 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
         int ip[K];
         bool act[K];
         double xi[K], yi[K], zi[K], hi2[K];
-        double ax[K], ay[K], az[K], pot[K];
+        double ax[K], ay[K], az[K], pot[K];  // this j-tile's sums
+        double sh[K][4];                     // compensated running sums: high parts (low: s_lo)
         double wlo[3] = {INFINITY, INFINITY, INFINITY}, whi[3] = {-INFINITY, -INFINITY, -INFINITY};
         double wh2 = 0.0;
 #pragma unroll
@@ -110,7 +120,11 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
             yi[k] = act[k] ? D.y[ip[k]] : FAR_POS;
             zi[k] = act[k] ? D.z[ip[k]] : -FAR_POS;
             hi2[k] = act[k] ? D.h2[ip[k]] : 0.0;
-            ax[k] = ay[k] = az[k] = pot[k] = 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                sh[k][c] = 0.0;
+                s_lo[c][k][tid] = 0.0;
+            }
             if (act[k]) {
                 wlo[0] = fmin(wlo[0], xi[k]); whi[0] = fmax(whi[0], xi[k]);
                 wlo[1] = fmin(wlo[1], yi[k]); whi[1] = fmax(whi[1], yi[k]);
@@ -127,6 +141,15 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
         }
         for (int o = 16; o > 0; o >>= 1) wh2 = fmax(wh2, __shfl_xor_sync(0xffffffffu, wh2, o));
         const bool warp_rows = wlo[0] <= whi[0];
+        // the warp's box in FP32, rounded outward, for the per-tile far test
+        // (FP32 keeps the test off the FP64 pipe, which the pair loop saturates)
+        float flo[3], fhi[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            flo[d] = warp_rows ? __double2float_rd(wlo[d]) : 0.f;
+            fhi[d] = warp_rows ? __double2float_ru(whi[d]) : 0.f;
+        }
+        const float fwh2 = __double2float_ru(wh2);
 
         for (int t = 0; t < ntile; t++) {
             const uint32_t gt = g + t;
@@ -135,22 +158,28 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
             if (ok && tid == 0) pending[s] = false;
             if (ok && warp_rows) {
                 const double *sx = s_src[s][0], *sy = s_src[s][1], *sz = s_src[s][2];
-                const double *sm = s_src[s][3], *sh = s_src[s][4];
+                const double *sm = s_src[s][3], *shj = s_src[s][4];
+#pragma unroll
+                for (int k = 0; k < K; k++) ax[k] = ay[k] = az[k] = pot[k] = 0.0;
                 // box test: the gap between the warp's rows and each record's
-                // box bounds r from below; far when it exceeds every H
+                // box bounds r from below; far when it exceeds every H.  In
+                // FP32 with the gap shrunk by 2^-20 of the coordinates'
+                // magnitude and the squared gap by 1e-5, which covers the
+                // roundings of the box arithmetic.
                 bool far = true;
 #pragma unroll
                 for (int r = 0; r < NMETA; r++) {
                     const JMeta M = s_meta[s][r];
                     if (M.ex < 0.f) continue;  // no particle
-                    const double c[3] = {M.cx, M.cy, M.cz}, e[3] = {M.ex, M.ey, M.ez};
-                    double d2 = 0.0;
+                    const float c[3] = {M.cx, M.cy, M.cz}, e[3] = {M.ex, M.ey, M.ez};
+                    float d2 = 0.f;
 #pragma unroll
                     for (int d = 0; d < 3; d++) {
-                        const double gap = fmax(0.0, fmax((c[d] - e[d]) - whi[d], wlo[d] - (c[d] + e[d])));
-                        d2 = fma(gap, gap, d2);
+                        const float slack = 9.5367e-7f * (fabsf(c[d]) + e[d] + fabsf(flo[d]) + fabsf(fhi[d]));
+                        const float gap = fmaxf(0.f, fmaxf((c[d] - e[d]) - fhi[d], flo[d] - (c[d] + e[d])) - slack);
+                        d2 = fmaf(gap, gap, d2);
                     }
-                    far = far && d2 * (1.0 - 1e-12) > fmax(wh2, (double)M.h2max);
+                    far = far && d2 > fmaxf(fwh2, M.h2max) * 1.00001f;
                 }
                 if (far) {
 #pragma unroll 2
@@ -172,7 +201,7 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
                 } else {
                     const int jt = W.jb + t * TJ;
                     for (int j = 0; j < TJ; j++) {
-                        const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j], hj = sh[j];
+                        const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j], hj = shj[j];
 #pragma unroll
                         for (int k = 0; k < K; k++) {
                             const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
@@ -195,6 +224,22 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
                         }
                     }
                 }
+                // the tile's sums (a few hundred terms, plain FP64) go into the
+                // row's compensated running sums: FP64 rounding then grows with
+                // the tile sums, not with a running sum over the whole j-range
+                // (which at a particle whose acceleration cancels is much
+                // larger than the result)
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const double tv[4] = {ax[k], ay[k], az[k], pot[k]};
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const double hsum = sh[k][c] + tv[c];
+                        const double bp = hsum - sh[k][c];
+                        s_lo[c][k][tid] += (sh[k][c] - (hsum - bp)) + (tv[c] - bp);
+                        sh[k][c] = hsum;
+                    }
+                }
             }
             // every thread is done with stage s (or a wait gave up)
             if (__syncthreads_or(!ok)) {
@@ -212,10 +257,10 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
         for (int k = 0; k < K; k++) {
             if (act[k]) {
                 const int li = warp * 32 * K + k * 32 + lane;
-                p[li] = ax[k];
-                p[ITILE + li] = ay[k];
-                p[2 * ITILE + li] = az[k];
-                p[3 * ITILE + li] = pot[k];
+                p[li] = sh[k][0] + s_lo[0][k][tid];
+                p[ITILE + li] = sh[k][1] + s_lo[1][k][tid];
+                p[2 * ITILE + li] = sh[k][2] + s_lo[2][k][tid];
+                p[3 * ITILE + li] = sh[k][3] + s_lo[3][k][tid];
             }
         }
     }
@@ -232,7 +277,9 @@ __global__ void __launch_bounds__(NT) k_fp64(ComputeArgs a)
     X(128, 1, 128, 3, "fp64_nt128_k1_tj128")        \
     X(128, 2, 128, 3, "fp64_nt128_k2_tj128")        \
     X(128, 4, 128, 3, "fp64_nt128_k4_tj128")        \
-    X(256, 1, 128, 3, "fp64_nt256_k1_tj128")
+    X(256, 1, 128, 3, "fp64_nt256_k1_tj128")        \
+    X(128, 2, 256, 3, "fp64_nt128_k2_tj256")        \
+    X(128, 4, 256, 3, "fp64_nt128_k4_tj256")
 
 #define SG_INFO(NT, K, TJ, NS, NAME) {0, NT, K, 1, TJ, 0, NAME, NT * K},
 static const VariantInfo kF64Variants[] = {SG_F64_VARIANTS(SG_INFO)};

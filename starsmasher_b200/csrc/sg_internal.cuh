@@ -83,10 +83,164 @@ __host__ __device__ inline double self_c(int nkernel)
 // particles give -c/2 * flag_{lower original index} * (m_j/H_i + m_j/H_j).
 struct PairOut { double ax, ay, az, pot; };
 
-// The CPU path divides (qq = 1/invq, amj/twohp, mj1/fourhp2); here the same
-// quantities come from reciprocals ih = 1/H = rsqrt(H^2): equal up to a last-
-// bit rounding, at a fraction of the FP64 cost.
-__device__ __forceinline__ void near_kernel_f64(int nkernel, double r2, double rinv,
+// The near-field pair evaluated with the CPU path's operations in the CPU
+// path's order (cpu_grav.f:71-157 nkernel 0, :187-268 nkernel 1, :298-375
+// nkernel 2): every product, sum, quotient and square root is an explicit
+// IEEE round-to-nearest operation (no contraction into FMA), so a near pair
+// gives the same bits as the CPU path does for the same r2, rinv, H.  Near
+// pairs are rare (r < max H), so their cost does not matter, and near q = 1
+// the kernel polynomials cancel by up to ~1e4: a last-bit difference in
+// their inputs would otherwise show as a ~1e-12 relative difference on a
+// particle whose acceleration cancels.
+#define SG_M(a, b) __dmul_rn((a), (b))
+#define SG_A(a, b) __dadd_rn((a), (b))
+#define SG_S(a, b) __dsub_rn((a), (b))
+#define SG_D(a, b) __ddiv_rn((a), (b))
+
+__device__ __forceinline__ void near_kernel_f64(int nkernel, double r2, double rinv, double amj,
+                                                double twohpi, double fourhpi2, double twohpj,
+                                                double fourhpj2, double mrinv1, double mrinv3,
+                                                double &gacc, double &gpot)
+{
+    const double invq1 = SG_M(rinv, twohpi), invq2 = SG_M(rinv, twohpj);
+    const double qq1 = SG_D(1.0, invq1), qq2 = SG_D(1.0, invq2);
+    const double q21 = SG_M(qq1, qq1), q22 = SG_M(qq2, qq2);
+    const double q31 = SG_M(qq1, q21), q32 = SG_M(qq2, q22);
+    const double invq21 = SG_M(invq1, invq1), invq22 = SG_M(invq2, invq2);
+    const double invq31 = SG_M(invq1, invq21), invq32 = SG_M(invq2, invq22);
+    const double mj11 = SG_D(amj, twohpi), mj12 = SG_D(amj, twohpj);
+    const double mj21 = SG_D(mj11, fourhpi2), mj22 = SG_D(mj12, fourhpj2);
+    const double g1 = (r2 <= fourhpi2) ? 1.0 : 0.0;
+    const double g2 = (r2 <= fourhpj2) ? 1.0 : 0.0;
+    double acc1, acc2, pot1, pot2;
+    // 0.5 * (g1 mj21 acc1 + (1 - g1) mrinv3 + g2 mj22 acc2 + (1 - g2) mrinv3), left to right
+    auto gsum = [&](double a1, double a2, double w1, double w2, double far1, double far2) {
+        double t = SG_M(SG_M(g1, w1), a1);
+        t = SG_A(t, far1);
+        t = SG_A(t, SG_M(SG_M(g2, w2), a2));
+        t = SG_A(t, far2);
+        return SG_M(0.5, t);
+    };
+    if (nkernel == 0) {
+        auto spline = [&](double q, double q2, double q3, double iq, double iq3, double &acc, double &pot) {
+            if (q < 0.5) {
+                acc = SG_A(10.666666666667, SG_M(q2, SG_S(SG_M(32.0, q), 38.4)));
+                pot = SG_A(-2.8, SG_M(q2, SG_A(5.333333333333, SG_M(q2, SG_S(SG_M(6.4, q), 9.6)))));
+            } else {
+                double a = SG_S(21.333333333333, SG_M(48.0, q));
+                a = SG_A(a, SG_M(38.4, q2));
+                a = SG_S(a, SG_M(10.666666666667, q3));
+                acc = SG_S(a, SG_M(0.066666666667, iq3));
+                const double inner =
+                    SG_A(10.666666666667,
+                         SG_M(q, SG_A(-16.0, SG_M(q, SG_S(9.6, SG_M(2.133333333333, q))))));
+                pot = SG_A(SG_A(-3.2, SG_M(0.066666666667, iq)), SG_M(q2, inner));
+            }
+        };
+        spline(qq1, q21, q31, invq1, invq31, acc1, pot1);
+        spline(qq2, q22, q32, invq2, invq32, acc2, pot2);
+        gacc = gsum(acc1, acc2, mj21, mj22, SG_M(SG_S(1.0, g1), mrinv3), SG_M(SG_S(1.0, g2), mrinv3));
+        double t = SG_M(SG_M(g1, mj11), pot1);
+        t = SG_A(t, SG_M(SG_S(g1, 1.0), mrinv1));
+        t = SG_A(t, SG_M(SG_M(g2, mj12), pot2));
+        t = SG_A(t, SG_M(SG_S(g2, 1.0), mrinv1));
+        gpot = SG_M(0.5, t);
+    } else {
+        auto wend = [&](double q, double q2, double g, double &acc, double &pot) {
+            if (nkernel == 1) {
+                double a = SG_A(-1515.9375, SG_M(195.0, q));
+                a = SG_A(5005.0, SG_M(q, a));
+                a = SG_A(-8957.8125, SG_M(q, a));
+                a = SG_A(9009.0, SG_M(q, a));
+                a = SG_A(-4379.375, SG_M(q, a));
+                a = SG_A(804.375, SG_M(q2, a));
+                a = SG_A(-187.6875, SG_M(q2, a));
+                acc = SG_A(28.4375, SG_M(q2, a));
+                double p = SG_A(-126.328125, SG_M(15.0, q));
+                p = SG_A(455.0, SG_M(q, p));
+                p = SG_A(-895.78125, SG_M(q, p));
+                p = SG_A(1001.0, SG_M(q, p));
+                p = SG_A(-547.421875, SG_M(q, p));
+                p = SG_A(134.0625, SG_M(q2, p));
+                p = SG_A(-46.921875, SG_M(q2, p));
+                p = SG_A(14.21875, SG_M(q2, p));
+                pot = g > 0.0 ? SG_A(-3.828125, SG_M(q2, p)) : 0.0;
+            } else {
+                double a = SG_A(-396.0, SG_M(65.625, q));
+                a = SG_A(962.5, SG_M(q, a));
+                a = SG_A(-1155.0, SG_M(q, a));
+                a = SG_A(618.75, SG_M(q, a));
+                a = SG_A(-115.5, SG_M(q2, a));
+                acc = SG_A(20.625, SG_M(q2, a));
+                double p = SG_A(-44.0, SG_M(6.5625, q));
+                p = SG_A(120.3125, SG_M(q, p));
+                p = SG_A(-165.0, SG_M(q, p));
+                p = SG_A(103.125, SG_M(q, p));
+                p = SG_A(-28.875, SG_M(q2, p));
+                p = SG_A(10.3125, SG_M(q2, p));
+                pot = g > 0.0 ? SG_A(-3.4375, SG_M(q2, p)) : 0.0;
+            }
+        };
+        wend(qq1, q21, g1, acc1, pot1);
+        wend(qq2, q22, g2, acc2, pot2);
+        gacc = gsum(acc1, acc2, mj21, mj22, SG_M(SG_S(1.0, g1), mrinv3), SG_M(SG_S(1.0, g2), mrinv3));
+        double t = SG_M(mj11, pot1);
+        t = SG_A(t, SG_M(SG_S(g1, 1.0), mrinv1));
+        t = SG_A(t, SG_M(mj12, pot2));
+        t = SG_A(t, SG_M(SG_S(g2, 1.0), mrinv1));
+        gpot = SG_M(0.5, t);
+    }
+}
+
+// FP64 pair of row slot ip and source slot jp given their separation dr
+// (x_j - x_i), the source mass and both H^2; the zero-distance rule reads
+// the flags and original indices of the sorted layout.  Evaluated like the
+// CPU path's row form: r2 summed without contraction, rinv = 1/sqrt(r2),
+// twohp = sqrt(H^2).
+static __device__ __forceinline__ PairOut pair_f64_core(const SortedF64 &D, int nkernel, int ip,
+                                                        int jp, double dr1, double dr2, double dr3,
+                                                        double amj, double fourhpi2,
+                                                        double fourhpj2)
+{
+    const double r2 = SG_A(SG_A(SG_M(dr1, dr1), SG_M(dr2, dr2)), SG_M(dr3, dr3));
+    double gacc, gpot;
+    if (r2 >= fmax(fourhpi2, fourhpj2)) {
+        const double rinv = SG_D(1.0, __dsqrt_rn(r2));
+        const double mrinv1 = SG_M(rinv, amj);
+        gacc = SG_M(SG_M(rinv, rinv), mrinv1);
+        gpot = -mrinv1;
+    } else if (r2 > 0.0) {
+        const double rinv = SG_D(1.0, __dsqrt_rn(r2));
+        const double mrinv1 = SG_M(rinv, amj);
+        const double mrinv3 = SG_M(SG_M(rinv, rinv), mrinv1);
+        near_kernel_f64(nkernel, r2, rinv, amj, __dsqrt_rn(fourhpi2), fourhpi2,
+                        __dsqrt_rn(fourhpj2), fourhpj2, mrinv1, mrinv3, gacc, gpot);
+    } else {
+        gacc = 0.0;
+        const double twohpi = __dsqrt_rn(fourhpi2), twohpj = __dsqrt_rn(fourhpj2);
+        const double s = SG_A(SG_D(amj, twohpi), SG_D(amj, twohpj));  // m/H_i + m/H_j
+        const double c = self_c(nkernel);
+        if (ip == jp) {
+            gpot = D.flag[ip] ? SG_M(-c, s) : 0.0;
+        } else {
+            const int lo = D.orig[ip] < D.orig[jp] ? ip : jp;
+            gpot = D.flag[lo] ? SG_M(SG_M(-0.5, c), s) : 0.0;
+        }
+    }
+    PairOut o;
+    o.ax = SG_M(gacc, dr1);
+    o.ay = SG_M(gacc, dr2);
+    o.az = SG_M(gacc, dr3);
+    o.pot = gpot;
+    return o;
+}
+
+// The same near-field formulas from reciprocals ih = 1/H = rsqrt(H^2) where
+// the CPU path divides (qq = 1/invq, amj/twohp, mj1/fourhp2), with
+// contraction allowed: equal to near_kernel_f64 up to last-bit roundings, at a
+// fraction of its cost and register use.  The split-FP32 kernel's near pairs
+// use it (their positions are the 48-bit hi + lo pairs anyway).
+__device__ __forceinline__ void near_kernel_fast(int nkernel, double r2, double rinv,
                                                 double amj, double ihi, double fourhpi2,
                                                 double ihj, double fourhpj2,
                                                 double mrinv1, double mrinv3,
@@ -142,10 +296,8 @@ __device__ __forceinline__ void near_kernel_f64(int nkernel, double r2, double r
     }
 }
 
-// FP64 pair of row slot ip and source slot jp given their separation dr
-// (x_j - x_i), the source mass and both H^2; the zero-distance rule reads
-// the flags and original indices of the sorted layout.
-static __device__ __forceinline__ PairOut pair_f64_core(const SortedF64 &D, int nkernel, int ip,
+// pair_f64_core with near_kernel_fast (the split-FP32 kernel's near pairs).
+static __device__ __forceinline__ PairOut pair_f64_fast(const SortedF64 &D, int nkernel, int ip,
                                                         int jp, double dr1, double dr2, double dr3,
                                                         double amj, double fourhpi2,
                                                         double fourhpj2)
@@ -161,7 +313,7 @@ static __device__ __forceinline__ PairOut pair_f64_core(const SortedF64 &D, int 
         const double rinv = rsqrt(r2);
         const double mrinv1 = rinv * amj;
         const double mrinv3 = rinv * rinv * mrinv1;
-        near_kernel_f64(nkernel, r2, rinv, amj, rsqrt(fourhpi2), fourhpi2, rsqrt(fourhpj2),
+        near_kernel_fast(nkernel, r2, rinv, amj, rsqrt(fourhpi2), fourhpi2, rsqrt(fourhpj2),
                         fourhpj2, mrinv1, mrinv3, gacc, gpot);
     } else {
         gacc = 0.0;

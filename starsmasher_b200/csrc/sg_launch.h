@@ -110,7 +110,7 @@ cudaError_t launch_wtile_out(const SetDesc *sets, const int *tile_set, int ntile
 // Plans the refine on the device from the per-set counts: for set s the rows
 // rlist[S.ioff, S.ioff + rcount[s]) in tiles of `itile` rows, every tile
 // split into the same number of j-chunks (enough items to fill `target`
-// persistent blocks, at least 1024 sources per chunk), one partial slot per
+// persistent blocks, at least 256 sources per chunk), one partial slot per
 // item.  Writes rsets (copies of sets with ni, ntiles, nchunks, slot_off of
 // the refine), the items and their count.  At most max_items items are
 // written; a plan that would need more sets DEVERR_INPUT (never expected:

@@ -36,33 +36,35 @@ static __device__ __noinline__ PairOut pair_f64_raw(const double *x, const doubl
                                                     const double *r2in, int nkernel, int i, int j)
 {
     const double dr1 = x[j] - x[i], dr2 = y[j] - y[i], dr3 = z[j] - z[i];
-    const double r2 = dr1 * dr1 + dr2 * dr2 + dr3 * dr3;
+    const double r2 = SG_A(SG_A(SG_M(dr1, dr1), SG_M(dr2, dr2)), SG_M(dr3, dr3));
     const double amj = m[j];
     const double fourhpi2 = fabs(r2in[i]), fourhpj2 = fabs(r2in[j]);
     double gacc, gpot;
     if (r2 >= fmax(fourhpi2, fourhpj2)) {
-        const double rinv = 1.0 / sqrt(r2);
-        const double mrinv1 = rinv * amj;
-        gacc = rinv * rinv * mrinv1;
+        const double rinv = SG_D(1.0, __dsqrt_rn(r2));
+        const double mrinv1 = SG_M(rinv, amj);
+        gacc = SG_M(SG_M(rinv, rinv), mrinv1);
         gpot = -mrinv1;
     } else if (r2 > 0.0) {
-        const double rinv = 1.0 / sqrt(r2);
-        const double mrinv1 = rinv * amj;
-        near_kernel_f64(nkernel, r2, rinv, amj, rsqrt(fourhpi2), fourhpi2, rsqrt(fourhpj2),
-                        fourhpj2, mrinv1, rinv * rinv * mrinv1, gacc, gpot);
+        const double rinv = SG_D(1.0, __dsqrt_rn(r2));
+        const double mrinv1 = SG_M(rinv, amj);
+        near_kernel_f64(nkernel, r2, rinv, amj, __dsqrt_rn(fourhpi2), fourhpi2,
+                        __dsqrt_rn(fourhpj2), fourhpj2, mrinv1, SG_M(SG_M(rinv, rinv), mrinv1),
+                        gacc, gpot);
     } else {
         gacc = 0.0;
-        const double twohpi = sqrt(fourhpi2), twohpj = sqrt(fourhpj2);
+        const double twohpi = __dsqrt_rn(fourhpi2), twohpj = __dsqrt_rn(fourhpj2);
+        const double s = SG_A(SG_D(amj, twohpi), SG_D(amj, twohpj));
         const double c = self_c(nkernel);
         if (i == j)
-            gpot = r2in[i] > 0.0 ? -c * (amj / twohpi + amj / twohpj) : 0.0;
+            gpot = r2in[i] > 0.0 ? SG_M(-c, s) : 0.0;
         else
-            gpot = r2in[min(i, j)] > 0.0 ? -0.5 * c * (amj / twohpi + amj / twohpj) : 0.0;
+            gpot = r2in[min(i, j)] > 0.0 ? SG_M(SG_M(-0.5, c), s) : 0.0;
     }
     PairOut o;
-    o.ax = gacc * dr1;
-    o.ay = gacc * dr2;
-    o.az = gacc * dr3;
+    o.ax = SG_M(gacc, dr1);
+    o.ay = SG_M(gacc, dr2);
+    o.az = SG_M(gacc, dr3);
     o.pot = gpot;
     return o;
 }

@@ -48,7 +48,7 @@ __device__ long long block_exclusive_scan(long long v, long long *total)
 // spread over many blocks (a listed row can have most of its set within its
 // softening length, e.g. a point-mass core, and pay the near-pair path for
 // most sources).
-constexpr int REFINE_MIN_J = 1024;
+constexpr int REFINE_MIN_J = 256;
 
 __device__ __forceinline__ int refine_chunks(const SetDesc &S, int tj, int nch_global)
 {

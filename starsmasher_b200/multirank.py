@@ -170,6 +170,27 @@ def forces_row_split_device(compute: DeviceRowCompute, own, n: int, group=None):
     return src, allgather_rows(out[:, lo:hi], n, group)
 
 
+class RowSplitStep:
+    """One gravity step of the reference's multi-GPU row split, as bench.py
+    times it: this rank owns rows [lo, hi) of one set of n particles
+    (main.f:283-295) and holds their (x, y, z, m, range2) in ``own``; each
+    call all-gathers the sources, evaluates the owned rows and all-gathers
+    the (4, n) result (forces_row_split_device)."""
+
+    def __init__(self, compute: DeviceRowCompute, own, n: int, group=None):
+        import torch.distributed as dist
+        self.compute, self.own, self.n, self.group = compute, own, n, group
+        self.lo, self.hi = gpu_row_range(n, dist.get_world_size(group), dist.get_rank(group))
+        if own.shape[1] != self.hi - self.lo:
+            raise ValueError(f"own holds {own.shape[1]} rows, the rank's slice is {self.hi - self.lo}")
+
+    def __call__(self, own=None):
+        """Returns (sources, result); ``own`` replaces the owned rows' data
+        (e.g. positions freshly copied from the host)."""
+        return forces_row_split_device(self.compute, self.own if own is None else own, self.n,
+                                       self.group)
+
+
 def gpu_compute_device(ctx, nkernel: int = 0, precision: str = "f32split") -> DeviceRowCompute:
     """Per-rank computation with the GPU library on device tensors, stream
     ordered: the library is pointed at torch's current stream, where the
@@ -179,7 +200,10 @@ def gpu_compute_device(ctx, nkernel: int = 0, precision: str = "f32split") -> De
     import torch
 
     def f(src, i_begin, ni, out):
-        ctx.set_stream(torch.cuda.current_stream(src.device).cuda_stream)
+        # torch's default stream reports handle 0, which the library reads as
+        # "the context's own stream"; pass cudaStreamLegacy (handle 1), the
+        # same default stream, instead
+        ctx.set_stream(torch.cuda.current_stream(src.device).cuda_stream or 1)
         n = src.shape[1]
         ctx.forces_device(n, src[0], src[1], src[2], src[3], src[4], out[0], out[1], out[2],
                           out[3], nkernel=nkernel, precision=precision, i_begin=i_begin, ni=ni)

@@ -15,7 +15,10 @@ ill-conditioned), as everywhere in these tests.  Tolerances:
 Rows checked against the oracle: every row of config 2 (the faithful
 triangle); for configs 3-5 a seeded sample per set plus the rows most likely
 to fail -- the smallest |a| (cancellation) and, for config 3, the point-mass
-core (row 0).
+core (row 0).  On the rows picked for their small |a| the FP64 bound also
+allows the rounding of an FP64 sum itself, |a - a_ref| <= 1e-12 |a_ref| +
+8 u sum_j |t_j| (u = 2^-53, t_j the pair terms): there the CPU path's own
+plain FP64 sums differ from the exact result by that much.
 """
 import numpy as np
 import pytest
@@ -55,11 +58,25 @@ def _amag(r):
 
 
 def _rows_for_set(a, b, amag, rng, nrand, nsmall):
-    """Seeded random rows of set [a, b) plus its nsmall smallest-|a| rows."""
+    """Seeded random rows of set [a, b) and, separately, its nsmall
+    smallest-|a| rows (global indices)."""
     n = b - a
     pick = rng.choice(n, min(n, nrand), replace=False)
     small = np.argsort(amag[a:b])[:nsmall]
-    return a + np.unique(np.concatenate([pick, small]))
+    return a + np.unique(pick), a + np.unique(small)
+
+
+def _abs_term_sum(ws, rows):
+    """sum_j m_j / r_ij^2 over the row's set (j != i): the scale of an FP64
+    sum's rounding error for that row."""
+    setid = np.searchsorted(ws.offsets, rows, side="right") - 1
+    out = np.zeros(len(rows))
+    for k, (g, s) in enumerate(zip(rows, setid)):
+        a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
+        d2 = (ws.x[a:b] - ws.x[g]) ** 2 + (ws.y[a:b] - ws.y[g]) ** 2 + (ws.z[a:b] - ws.z[g]) ** 2
+        d2[g - a] = np.inf
+        out[k] = np.sum(ws.m[a:b] / np.maximum(d2, 1e-300))
+    return out
 
 
 def _oracle_on_rows(ws, rows):
@@ -76,12 +93,16 @@ def _oracle_on_rows(ws, rows):
     return out
 
 
-def _check_rows(got, ref, rows, median_a, tol, what):
+def _check_rows(got, ref, rows, median_a, tol, what, abs_sum=None):
     """Relative errors on `rows` with the workload's median |a| as the
-    ill-conditioning reference."""
+    ill-conditioning reference; with abs_sum, the FP64 summation allowance
+    8 u abs_sum is added to the bound (see the module docstring)."""
     g = [np.asarray(x)[rows] for x in got]
     amag = _amag(ref)
-    e = np.sqrt(sum((g[q] - ref[q]) ** 2 for q in range(3))) / amag
+    num = np.sqrt(sum((g[q] - ref[q]) ** 2 for q in range(3)))
+    if abs_sum is not None:
+        num = np.maximum(0.0, num - 8 * 2.0 ** -53 * abs_sum)
+    e = num / amag
     ok = amag >= 1e-3 * median_a
     ep = np.abs(g[3] - ref[3]) / np.abs(ref[3])
     acc_max = float(e[ok].max()) if ok.any() else 0.0
@@ -126,10 +147,13 @@ def test_config3_sampled_rows_and_core(ctx):
     amag = _amag(r64)
     med = float(np.median(amag))
     rng = np.random.default_rng(33)
-    rows = np.unique(np.concatenate([[0], _rows_for_set(0, ws.n, amag, rng, 4096, 64)]))
-    ref = _oracle_on_rows(ws, rows)
-    _check_rows(r64, ref, rows, med, FP64_TOL, "config3 fp64 vs oracle")
-    _check_rows(r32, ref, rows, med, F32_TOL, "config3 f32split vs oracle")
+    rand, small = _rows_for_set(0, ws.n, amag, rng, 4096, 64)
+    rand = np.unique(np.concatenate([[0], rand]))
+    for rows, label in ((rand, "seeded rows + core"), (small, "smallest |a|")):
+        ref = _oracle_on_rows(ws, rows)
+        S = _abs_term_sum(ws, rows) if label == "smallest |a|" else None
+        _check_rows(r64, ref, rows, med, FP64_TOL, f"config3 fp64 vs oracle, {label}", S)
+        _check_rows(r32, ref, rows, med, F32_TOL, f"config3 f32split vs oracle, {label}")
     r = err_report(*r32, *r64)
     print("config3 f32split vs fp64, all rows", r)
     assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
@@ -147,11 +171,14 @@ def test_config4_all_64_models(ctx):
     amag = _amag(r64)
     med = float(np.median(amag))
     rng = np.random.default_rng(44)
-    rows = np.concatenate([_rows_for_set(int(ws.offsets[s]), int(ws.offsets[s + 1]), amag, rng,
-                                         128, 8) for s in range(ws.nsets)])
-    ref = _oracle_on_rows(ws, rows)
-    _check_rows(r64, ref, rows, med, FP64_TOL, "config4 fp64 vs oracle")
-    _check_rows(r32, ref, rows, med, F32_TOL, "config4 f32split vs oracle")
+    picks = [_rows_for_set(int(ws.offsets[s]), int(ws.offsets[s + 1]), amag, rng, 128, 8)
+             for s in range(ws.nsets)]
+    for k, label in ((0, "seeded rows"), (1, "smallest |a|")):
+        rows = np.concatenate([p[k] for p in picks])
+        ref = _oracle_on_rows(ws, rows)
+        S = _abs_term_sum(ws, rows) if k == 1 else None
+        _check_rows(r64, ref, rows, med, FP64_TOL, f"config4 fp64 vs oracle, {label}", S)
+        _check_rows(r32, ref, rows, med, F32_TOL, f"config4 f32split vs oracle, {label}")
     r = err_report(*r32, *r64)
     print("config4 f32split vs fp64, all rows", r)
     assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
@@ -189,11 +216,16 @@ def test_config5_graph_sweep_first_and_last_call(ctx):
             med = float(np.median(amag))
             pos = [x.cpu().numpy() for x in X]
             kicked = inputs.ParticleSets(pos[0], pos[1], pos[2], pos[3], pos[4], ws.offsets)
-            rows = np.concatenate([_rows_for_set(int(ws.offsets[s]), int(ws.offsets[s + 1]), amag,
-                                                 rng, 64, 8) for s in range(ws.nsets)])
-            ref = _oracle_on_rows(kicked, rows)
-            _check_rows(r64, ref, rows, med, FP64_TOL, f"config5 call {call} fp64 vs oracle")
-            _check_rows(r32, ref, rows, med, F32_TOL, f"config5 call {call} f32split vs oracle")
+            picks = [_rows_for_set(int(ws.offsets[s]), int(ws.offsets[s + 1]), amag, rng, 64, 8)
+                     for s in range(ws.nsets)]
+            for k, label in ((0, "seeded rows"), (1, "smallest |a|")):
+                rows = np.concatenate([p[k] for p in picks])
+                ref = _oracle_on_rows(kicked, rows)
+                S = _abs_term_sum(kicked, rows) if k == 1 else None
+                _check_rows(r64, ref, rows, med, FP64_TOL,
+                            f"config5 call {call} fp64 vs oracle, {label}", S)
+                _check_rows(r32, ref, rows, med, F32_TOL,
+                            f"config5 call {call} f32split vs oracle, {label}")
             r = err_report(*r32, *r64)
             print(f"config5 call {call} f32split vs fp64, all rows", r)
             assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r

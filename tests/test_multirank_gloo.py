@@ -97,7 +97,11 @@ def _worker_device(rank, world, port, q):
         s = inputs.single_polytrope(701, 1.5, seed=3)
         lo, hi = multirank.gpu_row_range(s.n, world, rank)
         own = torch.from_numpy(np.stack([a[lo:hi] for a in (s.x, s.y, s.z, s.m, s.range2)]))
-        src, res = multirank.forces_row_split_device(_oracle_compute_tensor, own, s.n)
+        # the step bench.py times, twice in a row (the second from fresh
+        # owned data, as its end-to-end form does)
+        step = multirank.RowSplitStep(_oracle_compute_tensor, own, s.n)
+        step()
+        src, res = step(own.clone())
         q.put((rank, src.numpy(), res.numpy()))
     finally:
         dist.destroy_process_group()
