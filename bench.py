@@ -77,6 +77,10 @@ def parse():
                         "(seeded 1e-3 position kick + gravity) on device-resident state")
     p.add_argument("--no-separate", action="store_true",
                    help="batched workloads: skip the one-call-per-set comparison")
+    p.add_argument("--l2-flush", default="write", choices=["write", "read"],
+                   help="L2 flush before every timed step: write 256 MB (default), or read "
+                        "512 MB, which evicts without leaving dirty lines for the next "
+                        "kernel to write back (for DRAM-traffic captures)")
     p.add_argument("--tree-thetas", default="0.3,0.5",
                    help="single-set workloads: opening angles of the Barnes-Hut tree "
                         "section ('' skips it); accuracy against the FP64 kernel")
@@ -256,18 +260,26 @@ def run_reference_arm(args, world, rank):
 
 class Timer:
     """CUDA-event timing of steps on one stream, with an L2 flush (a 256 MB
-    write, > 126 MB of L2) before every timed step."""
+    write, > 126 MB of L2; or a 512 MB read) before every timed step."""
 
-    def __init__(self, torch, stream, device):
+    def __init__(self, torch, stream, device, mode="write"):
         self.torch = torch
         self.stream = stream
-        self.flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")
+        self.mode = mode
+        n = (64 if mode == "write" else 128) * 1024 * 1024
+        self.flush = torch.ones(n, dtype=torch.float32, device=f"cuda:{device}")
+
+    def do_flush(self):
+        if self.mode == "write":
+            self.flush.zero_()
+        else:
+            self.flush.sum()
 
     def run(self, fn, steps):
         torch = self.torch
         evs = []
         for _ in range(steps):
-            self.flush.zero_()
+            self.do_flush()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(self.stream)
@@ -406,7 +418,7 @@ def main():
         ctx.set_fp64_band(args.fp64_band)
     if args.refine is not None:
         ctx.set_refine(args.refine)
-    timer = Timer(torch, stream, device)
+    timer = Timer(torch, stream, device, args.l2_flush)
 
     X, outs = upload(torch, ws, device)
     W = torch.empty(ws.nsets, dtype=torch.float64, device=f"cuda:{device}")
@@ -683,7 +695,8 @@ def main():
                        "precision": args.precision, "nkernel": args.nkernel,
                        "fp64_band": args.fp64_band if args.fp64_band is not None else "library default",
                        "refine": args.refine if args.refine is not None else "library default",
-                       "l2": "flushed before every timed step (256 MB write)",
+                       "l2": ("flushed before every timed step (256 MB write)" if args.l2_flush == "write"
+                              else "flushed before every timed step (512 MB read)"),
                        "parallelism": mode},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "fp64": fp64, "accuracy_vs_fp64": acc, "refined_rows": refined,

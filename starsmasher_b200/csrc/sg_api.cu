@@ -136,7 +136,18 @@ struct Plan {
     int grid = 1, nchunks_max = 1;
     std::vector<SetDesc> sets;
     std::vector<int> tile_set, meta_set;
+    std::vector<int2> tile_slots;  // per i-tile: first partial slot, j-chunk count
     std::vector<WorkItem> items;
+    // set of global i-tile t (binary search over the sets' tile offsets)
+    int tile_set_of(int t) const
+    {
+        int lo = 0, hi = nsets - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (sets[mid].tile_off <= t) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+    }
 };
 
 // A captured graph bakes in the context's work plan and buffer addresses.
@@ -177,6 +188,7 @@ struct sphgrav_ctx {
     DBuf<float> f32;    // 8 * pcap
     size_t pcap = 0;
     DBuf<SetDesc> sets;
+    DBuf<int2> tile_slots;
     DBuf<ITileMeta> imeta;
     DBuf<JMeta> jmeta;
     DBuf<WorkItem> items;
@@ -398,6 +410,49 @@ static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
             if (eff > best + 1e-9) { best = eff; single_nch = nch; }
         }
     }
+    // Chunk counts per i-tile.  Few tiles (<= 2 waves of persistent CTAs),
+    // or the FP64 kernel: every tile of a set gets the same count, enough
+    // items for the queue to balance (one set: the count that fills the last
+    // wave best).  Split-FP32 with many tiles: every tile is one whole-j-range
+    // item, except the TAIL_DIV-th part of a wave of tiles that comes last
+    // in the longest-first order, which is cut into 4 chunks: the queue still
+    // ends on small items, and the FP64 partial sums (written per item,
+    // merged by k_merge) stay about the size of the outputs instead of 4x.
+    // (The FP64 kernel keeps chunks everywhere: a row tile holding a point
+    // mass with a large H, like the red giant's core, pays the serial near-
+    // pair path for most of the set and must not be one item.)
+    constexpr int TAIL_DIV = 2, TAIL_CHUNKS = 4;
+    std::vector<int> tile_nch(P.ntiles, 1);
+    auto set_maxch = [&](const SetDesc &d) {
+        const int jtiles = (d.n + P.tj - 1) / P.tj;
+        return std::max(1, std::min(jtiles, (int)(((long long)jtiles * P.tj) / kMinChunkJ)));
+    };
+    if (P.ntiles <= 2 * resident || precision != SPHGRAV_F32SPLIT) {
+        for (int s = 0; s < P.nsets; s++) {
+            const SetDesc &d = P.sets[s];
+            int nch = P.ntiles > 0 ? (target + P.ntiles - 1) / P.ntiles : 1;
+            nch = std::max(1, std::min(nch, set_maxch(d)));
+            if (single_nch > 0) nch = single_nch;
+            for (int t = 0; t < d.ntiles; t++) tile_nch[d.tile_off + t] = nch;
+        }
+    } else {
+        // whole-tile costs, longest first (stable: ties keep set and tile order)
+        std::vector<std::pair<long long, int>> order;
+        order.reserve(P.ntiles);
+        for (const SetDesc &d : P.sets)
+            for (int t = 0; t < d.ntiles; t++)
+                order.push_back({(long long)std::min(P.itile, d.ni - t * P.itile) * d.npad,
+                                 d.tile_off + t});
+        std::stable_sort(order.begin(), order.end(),
+                         [](const std::pair<long long, int> &a, const std::pair<long long, int> &b) {
+                             return a.first > b.first;
+                         });
+        const int tail = std::max(1, resident / TAIL_DIV);
+        for (int k = P.ntiles - tail; k < P.ntiles; k++) {
+            const int t = order[k].second;
+            tile_nch[t] = std::min(TAIL_CHUNKS, set_maxch(P.sets[P.tile_set_of(t)]));
+        }
+    }
     int slot = 0;
     P.nchunks_max = 1;
     struct Cost { long long cost; WorkItem w; };
@@ -405,27 +460,27 @@ static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     for (int s = 0; s < P.nsets; s++) {
         SetDesc &d = P.sets[s];
         const int jtiles = (d.n + P.tj - 1) / P.tj;
-        int nch = P.ntiles > 0 ? (target + P.ntiles - 1) / P.ntiles : 1;
-        const int maxch = std::max(1, (int)(((long long)jtiles * P.tj) / kMinChunkJ));
-        nch = std::max(1, std::min(nch, std::min(maxch, std::max(1, jtiles))));
-        if (single_nch > 0) nch = single_nch;
-        d.nchunks = nch;
+        d.nchunks = 1;
         d.slot_off = slot;
-        slot += d.ntiles * nch;
-        P.nchunks_max = std::max(P.nchunks_max, nch);
         for (int t = 0; t < d.ntiles; t++) {
             const int rows = std::min(P.itile, d.ni - t * P.itile);
+            const int nch = tile_nch[d.tile_off + t];
+            P.tile_slots.push_back({slot, nch});
+            d.nchunks = std::max(d.nchunks, nch);
             for (int ch = 0; ch < nch; ch++) {
                 WorkItem w;
                 memset(&w, 0, sizeof(w));
                 w.set = s;
                 w.tile = t;
                 w.chunk = ch;
+                w.slot = slot + ch;
                 w.jb = (int)((long long)jtiles * ch / nch) * P.tj;
                 w.je = (int)((long long)jtiles * (ch + 1) / nch) * P.tj;
                 items.push_back({(long long)rows * (w.je - w.jb), w});
             }
+            slot += nch;
         }
+        P.nchunks_max = std::max(P.nchunks_max, d.nchunks);
         for (int t = 0; t < d.ntiles; t++) P.tile_set.push_back(s);
         for (int r = 0; r < d.npad / META_J; r++) P.meta_set.push_back(s);
     }
@@ -464,13 +519,17 @@ static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_ro
         ++c->epoch;  // graphs captured under the old plan must not replay
         TRY(ensure(c, c->sets, std::max(1, P.nsets), "sets"));
         TRY(ensure(c, c->tile_set, std::max(1, P.ntiles), "tile_set"));
+        TRY(ensure(c, c->tile_slots, std::max(1, P.ntiles), "tile_slots"));
         TRY(ensure(c, c->meta_set, std::max(1, P.nmeta), "meta_set"));
         TRY(ensure(c, c->items, std::max(1, P.nitems), "items"));
         CUDA_TRY(cudaMemcpyAsync(c->sets.p, P.sets.data(), sizeof(SetDesc) * P.nsets,
                                  cudaMemcpyHostToDevice, c->stream));
-        if (P.ntiles)
+        if (P.ntiles) {
             CUDA_TRY(cudaMemcpyAsync(c->tile_set.p, P.tile_set.data(), sizeof(int) * P.ntiles,
                                      cudaMemcpyHostToDevice, c->stream));
+            CUDA_TRY(cudaMemcpyAsync(c->tile_slots.p, P.tile_slots.data(), sizeof(int2) * P.ntiles,
+                                     cudaMemcpyHostToDevice, c->stream));
+        }
         if (P.nmeta)
             CUDA_TRY(cudaMemcpyAsync(c->meta_set.p, P.meta_set.data(), sizeof(int) * P.nmeta,
                                      cudaMemcpyHostToDevice, c->stream));
@@ -808,8 +867,8 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
         CUDA_TRY(cudaMemsetAsync(c->rcount.p, 0, sizeof(int) * P.nsets, st));
     }
     c->refine_nsets = refine ? P.nsets : 0;
-    CUDA_TRY(launch_merge(c->sets.p, c->tile_set.p, P.ntiles, P.itile, c->ilist.p, D,
-                          c->partials.p, out, refine ? nullptr : c->wtile.p, R, st));
+    CUDA_TRY(launch_merge(c->sets.p, c->tile_set.p, c->tile_slots.p, P.ntiles, P.itile, c->ilist.p,
+                          D, c->partials.p, out, refine ? nullptr : c->wtile.p, R, st));
     if (refine) TRY(run_refine(c, nkernel, D, out));
     if (W && refine)
         CUDA_TRY(launch_wtile_out(c->sets.p, c->tile_set.p, P.ntiles, P.itile, c->ilist.p, D,
@@ -1039,7 +1098,8 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->graphs.clear();
     c->in.release(); c->out.release(); c->keys_in.release(); c->keys_out.release();
     c->bbox.release(); c->vals_in.release(); c->vals_out.release(); c->ilist.release();
-    c->nsel.release(); c->tile_set.release(); c->meta_set.release(); c->head.release();
+    c->nsel.release(); c->tile_set.release(); c->tile_slots.release(); c->meta_set.release();
+    c->head.release();
     c->err.release(); c->sort_temp.release(); c->sel_temp.release(); c->d64.release();
     c->orig.release(); c->flag.release(); c->f32.release(); c->sets.release();
     c->imeta.release(); c->jmeta.release(); c->items.release(); c->partials.release();

@@ -645,7 +645,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
             if (!failed) {
                 // combine the Q threads of a row (fixed order), convert, write FP64 partials
                 __syncwarp();
-                const size_t slot = (size_t)(S.slot_off + Wk.tile * S.nchunks + Wk.chunk);
+                const size_t slot = (size_t)Wk.slot;
                 double *p = a.partials + slot * 4 * ITILE;
                 if (a.gpart) {
 #pragma unroll

@@ -25,8 +25,8 @@ struct SetDesc {
     int tile_off;  // first i-tile of the set (global i-tile index)
     int ntiles;    // i-tiles of the set
     int meta_off;  // first j metadata record of the set
-    int slot_off;  // first partial slot of the set (in i-tile partial blocks)
-    int nchunks;   // j-chunks per i-tile
+    int slot_off;  // first partial slot of the set (refine plans: of its items)
+    int nchunks;   // j-chunks per i-tile (the main plan: the most of any tile)
 };
 
 // One unit of the persistent kernels' device-side queue.
@@ -35,7 +35,8 @@ struct WorkItem {
     int tile;    // set-local i-tile
     int jb, je;  // set-local sorted slots [jb, je), multiples of the j-tile
     int chunk;   // j-chunk index within the i-tile
-    int pad_[3];
+    int slot;    // partial-sum slot of this item
+    int pad_[2];
 };
 
 // Padded, spatially sorted SoA copies of the inputs.
@@ -239,7 +240,8 @@ static __device__ __forceinline__ PairOut pair_f64_core(const SortedF64 &D, int 
 // the CPU path divides (qq = 1/invq, amj/twohp, mj1/fourhp2), with
 // contraction allowed: equal to near_kernel_f64 up to last-bit roundings, at a
 // fraction of its cost and register use.  The split-FP32 kernel's near pairs
-// use it (their positions are the 48-bit hi + lo pairs anyway).
+// (their positions are the 48-bit hi + lo pairs anyway) and the tree mode (an
+// approximation) use it.
 __device__ __forceinline__ void near_kernel_fast(int nkernel, double r2, double rinv,
                                                 double amj, double ihi, double fourhpi2,
                                                 double ihj, double fourhpj2,

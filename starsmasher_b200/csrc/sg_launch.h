@@ -58,7 +58,7 @@ struct ComputeArgs {
     const int *ilist;
     const ITileMeta *imeta;
     const JMeta *jmeta;
-    double *partials;    // [slot][4][itile]
+    double *partials;    // [slot][4][itile], slot = WorkItem::slot
     // split-FP32: [slot][itile] sum over the item's j-tiles of |FP32 tile sum|^2
     // (acceleration components, both packed lanes): the scale of the FP32
     // rounding error of the row, merged into the refine test (nullable)
@@ -99,9 +99,11 @@ struct MergeRefine {
     int *rlist = nullptr;          // listed sorted slots; set s at [S.ioff, S.ioff + S.ni)
     double *scale = nullptr;       // optional: G per row in the caller's order
 };
-cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, int ntiles_total, int itile,
-                         const int *ilist, const SortedF64 D, const double *partials,
-                         OutputsDev out, double *wtile, const MergeRefine &R, cudaStream_t st);
+// tile_slots[t] = (first partial slot, j-chunk count) of global i-tile t.
+cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, const int2 *tile_slots,
+                         int ntiles_total, int itile, const int *ilist, const SortedF64 D,
+                         const double *partials, OutputsDev out, double *wtile,
+                         const MergeRefine &R, cudaStream_t st);
 cudaError_t launch_wtile_out(const SetDesc *sets, const int *tile_set, int ntiles_total, int itile,
                              const int *ilist, const SortedF64 D, const double *pot, double *wtile,
                              cudaStream_t st);

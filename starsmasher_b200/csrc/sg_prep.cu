@@ -460,13 +460,14 @@ __device__ double block_sum_fixed(double w)
 // Split-FP32 calls also merge the rows' error scales G^2 (sum over j-tiles of
 // |FP32 tile sum|^2) and append every row with G^2 > thresh2 |a|^2 to its
 // set's refine list, rlist[S.ioff + k], k counted in rcount[set].
-__global__ void k_merge(const SetDesc *sets, const int *tile_set, int itile, const int *ilist,
-                        SortedF64 D, const double *partials, OutputsDev out, double *wtile,
-                        MergeRefine R)
+__global__ void k_merge(const SetDesc *sets, const int *tile_set, const int2 *tile_slots, int itile,
+                        const int *ilist, SortedF64 D, const double *partials, OutputsDev out,
+                        double *wtile, MergeRefine R)
 {
     const int t = blockIdx.x;
     const int set = tile_set[t];
     const SetDesc S = sets[set];
+    const int2 ts = tile_slots[t];  // first partial slot, j-chunks of this tile
     const int lt = t - S.tile_off;
     const int r0 = lt * itile;
     const int nrow = min(itile, S.ni - r0);
@@ -474,8 +475,8 @@ __global__ void k_merge(const SetDesc *sets, const int *tile_set, int itile, con
     for (int li = threadIdx.x; li < nrow; li += blockDim.x) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         float g2 = 0.f;
-        for (int c = 0; c < S.nchunks; c++) {
-            const size_t slot = (size_t)(S.slot_off + lt * S.nchunks + c);
+        for (int c = 0; c < ts.y; c++) {
+            const size_t slot = (size_t)(ts.x + c);
             const double *p = partials + slot * 4 * itile;
 #pragma unroll
             for (int q = 0; q < 4; q++) acc[q] += p[q * itile + li];
@@ -501,12 +502,14 @@ __global__ void k_merge(const SetDesc *sets, const int *tile_set, int itile, con
     if (threadIdx.x == 0 && wtile) wtile[t] = wt;
 }
 
-cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, int ntiles_total, int itile,
-                         const int *ilist, const SortedF64 D, const double *partials,
-                         OutputsDev out, double *wtile, const MergeRefine &R, cudaStream_t st)
+cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, const int2 *tile_slots,
+                         int ntiles_total, int itile, const int *ilist, const SortedF64 D,
+                         const double *partials, OutputsDev out, double *wtile,
+                         const MergeRefine &R, cudaStream_t st)
 {
     if (ntiles_total <= 0) return cudaSuccess;
-    k_merge<<<ntiles_total, 256, 0, st>>>(sets, tile_set, itile, ilist, D, partials, out, wtile, R);
+    k_merge<<<ntiles_total, 256, 0, st>>>(sets, tile_set, tile_slots, itile, ilist, D, partials,
+                                          out, wtile, R);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -540,22 +543,25 @@ cudaError_t launch_wtile_out(const SetDesc *sets, const int *tile_set, int ntile
     return cudaGetLastError();
 }
 
-// W = 1/2 sum m_i phi_i per set (output.f:232-252), summed over the set's
-// tiles in tile order.
+// W = 1/2 sum m_i phi_i per set (output.f:232-252): one block per set sums
+// the set's tile sums, thread k over tiles k, k + blockDim, ... in order,
+// then a fixed tree over the threads.
 __global__ void k_wsum(const SetDesc *sets, int nsets, const double *wtile, double *W)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.x;
     if (s >= nsets) return;
     const SetDesc S = sets[s];
     double w = 0.0;
-    for (int t = 0; t < S.ntiles; t++) w += wtile[S.tile_off + t];
-    W[s] = 0.5 * w;
+    for (int t = threadIdx.x; t < S.ntiles; t += blockDim.x) w += wtile[S.tile_off + t];
+    const double tot = block_sum_fixed(w);
+    if (threadIdx.x == 0) W[s] = 0.5 * tot;
 }
 
 cudaError_t launch_wsum(const SetDesc *sets, int nsets, const double *wtile, double *W,
                         cudaStream_t st)
 {
-    k_wsum<<<grid_for(nsets, 128, 1 << 20), 128, 0, st>>>(sets, nsets, wtile, W);
+    if (nsets <= 0) return cudaSuccess;
+    k_wsum<<<nsets, 128, 0, st>>>(sets, nsets, wtile, W);
     ++g_launches;
     return cudaGetLastError();
 }

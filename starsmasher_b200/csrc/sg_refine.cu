@@ -90,29 +90,44 @@ __global__ void __launch_bounds__(PLAN_NT) k_refine_plan(const SetDesc *sets, in
         }
         return;
     }
+    // pass 3: the refine descriptors of this thread's sets (slot_off = the
+    // set's first item)
     for (int s = s0; s < s1; s++) {
         SetDesc S = sets[s];
         const int r = min(rcount[s], S.ni);
         const int nt = (r + itile - 1) / itile;
         const int nch = refine_chunks(S, tj, nch_global);
-        const int jtiles = (S.n + tj - 1) / tj;
         S.ni = r;
         S.ntiles = nt;
         S.nchunks = nch;
         S.slot_off = (int)base;
         rsets[s] = S;
-        for (int it = 0; it < nt; it++)
-            for (int c = 0; c < nch; c++) {
-                WorkItem w;
-                w.set = s;
-                w.tile = it;
-                w.chunk = c;
-                w.jb = (int)((long long)jtiles * c / nch) * tj;
-                w.je = (int)((long long)jtiles * (c + 1) / nch) * tj;
-                w.pad_[0] = w.pad_[1] = w.pad_[2] = 0;
-                items[base + (long long)it * nch + c] = w;
-            }
         base += (long long)nt * nch;
+    }
+    __syncthreads();  // rsets visible to the whole block
+    // pass 4: the items, spread over all threads (one set can own them all):
+    // item k belongs to the last set whose slot_off <= k (a set without
+    // items has the slot_off of the next set that has some, so the last
+    // such set is never empty)
+    for (long long k = t; k < total_items; k += blockDim.x) {
+        int lo = 0, hi = nsets - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (rsets[mid].slot_off <= k) lo = mid; else hi = mid - 1;
+        }
+        const SetDesc S = rsets[lo];
+        const int local = (int)(k - S.slot_off);
+        const int it = local / S.nchunks, c = local - it * S.nchunks;
+        const int jtiles = (S.n + tj - 1) / tj;
+        WorkItem w;
+        w.set = lo;
+        w.tile = it;
+        w.chunk = c;
+        w.slot = (int)k;  // = S.slot_off + it * S.nchunks + c
+        w.jb = (int)((long long)jtiles * c / S.nchunks) * tj;
+        w.je = (int)((long long)jtiles * (c + 1) / S.nchunks) * tj;
+        w.pad_[0] = w.pad_[1] = 0;
+        items[k] = w;
     }
     if (t == 0) *nitems = (int)total_items;
 }
@@ -127,6 +142,8 @@ cudaError_t launch_refine_plan(const SetDesc *sets, int nsets, const int *rcount
     return cudaGetLastError();
 }
 
+// One warp per refined row: lane l sums chunks l, l + 32, ... in order, then
+// a fixed shuffle tree combines the lanes (deterministic).
 __global__ void k_refine_merge(const SetDesc *sets, const SetDesc *rsets, const int *tile_set,
                                int itile_main, int itile_ref, const int *rcount, const int *rlist,
                                SortedF64 D, const double *rpart, OutputsDev out)
@@ -139,19 +156,25 @@ __global__ void k_refine_merge(const SetDesc *sets, const SetDesc *rsets, const 
     const int l0 = lt * itile_main, l1 = min(r, l0 + itile_main);
     if (l0 >= l1) return;
     const SetDesc RS = rsets[set];
-    for (int li = l0 + threadIdx.x; li < l1; li += blockDim.x) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int li = l0 + warp; li < l1; li += nw) {
         const int rt = li / itile_ref, ri = li - rt * itile_ref;
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int c = 0; c < RS.nchunks; c++) {
+        for (int c = lane; c < RS.nchunks; c += 32) {
             const double *p = rpart + (size_t)(RS.slot_off + rt * RS.nchunks + c) * 4 * itile_ref;
 #pragma unroll
             for (int q = 0; q < 4; q++) acc[q] += p[q * itile_ref + ri];
         }
-        const int o = D.orig[rlist[S.ioff + li]];
-        out.ax[o] = acc[0];
-        out.ay[o] = acc[1];
-        out.az[o] = acc[2];
-        out.pot[o] = acc[3];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        if (lane == 0) {
+            const int o = D.orig[rlist[S.ioff + li]];
+            out.ax[o] = acc[0];
+            out.ay[o] = acc[1];
+            out.az[o] = acc[2];
+            out.pot[o] = acc[3];
+        }
     }
 }
 

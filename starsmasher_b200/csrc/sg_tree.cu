@@ -25,7 +25,7 @@
 //     particles of opened leaves that lie farther than every H from the
 //     group's box are Newtonian FP32 pairs without a per-pair test, the
 //     others are tested pair by pair: FP32 when Newtonian, FP64 with the
-//     CPU-path formulas (pair_f64_core) for r < max(H_i, H_j) and r = 0;
+//     CPU-path formulas (pair_f64_fast) for r < max(H_i, H_j) and r = 0;
 //   * a group with more than TREE_BUDGET tested particles (a dense region
 //     inside a softening sphere, e.g. a point-mass core with a large H)
 //     leaves the walk and gets the direct FP64 sum over all particles
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
             if (lane < cnt) {
                 const int o = q[lane] >> 8, e = q[lane] & 255;
                 const int si = s0 + o, j = ps[e];
-                const PairOut r = pair_f64_core(D, a.nkernel, si, j, D.x[j] - D.x[si],
+                const PairOut r = pair_f64_fast(D, a.nkernel, si, j, D.x[j] - D.x[si],
                                                 D.y[j] - D.y[si], D.z[j] - D.z[si], D.m[j],
                                                 D.h2[si], D.h2[j]);
                 qr[0][lane] = r.ax;
@@ -690,7 +690,7 @@ k_tree_heavy(const int *heavy, const int2 *groups, SortedF64 D, int n, int nkern
     if (act) {
         const double xi = D.x[si], yi = D.y[si], zi = D.z[si], h2i = D.h2[si];
         for (int j = jb + w; j < je; j += HEAVY_WARPS) {
-            const PairOut o = pair_f64_core(D, nkernel, si, j, D.x[j] - xi, D.y[j] - yi,
+            const PairOut o = pair_f64_fast(D, nkernel, si, j, D.x[j] - xi, D.y[j] - yi,
                                             D.z[j] - zi, D.m[j], h2i, D.h2[j]);
             sx += o.ax;
             sy += o.ay;
