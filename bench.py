@@ -81,6 +81,9 @@ def parse():
                    help="L2 flush before every timed step: write 256 MB (default), or read "
                         "512 MB, which evicts without leaving dirty lines for the next "
                         "kernel to write back (for DRAM-traffic captures)")
+    p.add_argument("--phases", action="store_true",
+                   help="load the diagnostic build (python -m starsmasher_b200.build --phases) and "
+                        "report the split-FP32 kernel's cycles per phase over 2 extra calls")
     p.add_argument("--tree-thetas", default="0.3,0.5",
                    help="single-set workloads: opening angles of the Barnes-Hut tree "
                         "section ('' skips it); accuracy against the FP64 kernel")
@@ -290,6 +293,23 @@ class Timer:
         return sum(a.elapsed_time(b) for a, b in evs) / max(1, steps)
 
 
+def phase_shares(ph):
+    """Shares of consumer-warp and producer-warp cycles per phase, and the
+    tile counts, from Context.phase_read()."""
+    cons = ("item", "rows", "wait_full", "far", "checked", "near", "end")
+    prod = ("producer_wait", "producer_work")
+    ct = sum(ph[k] for k in cons) or 1
+    pt = sum(ph[k] for k in prod) or 1
+    nf, nc = ph["n_far"], ph["n_checked"]
+    return {"consumer_share": {k: ph[k] / ct for k in cons},
+            "producer_share": {k: ph[k] / pt for k in prod},
+            "checked_tile_fraction": nc / max(1, nf + nc),
+            "cycles_per_far_tile": ph["far"] / max(1, nf),
+            "cycles_per_checked_tile": ph["checked"] / max(1, nc),
+            "near_eval_calls": ph["n_near"], "items_per_consumer_warp_total": ph["n_items"],
+            "raw": ph}
+
+
 def upload(torch, ws, device):
     dt = torch.float64
     X = [torch.as_tensor(a).to(device=f"cuda:{device}", dtype=dt)
@@ -392,6 +412,8 @@ def main():
     import torch.distributed as dist
     from datetime import timedelta
 
+    if args.phases:
+        os.environ["SPHGRAV_B200_BUILD"] = "phases"
     from starsmasher_b200 import Context, api, launch_count, multirank
 
     if world > 1:
@@ -679,6 +701,18 @@ def main():
         extras["config4_batched"] = config4_section(torch, ctx, timer, device, args)
         extras["config5_graph_sweep"] = config5_section(torch, ctx, timer, stream, device, args)
 
+    phases = None
+    if args.phases and args.precision == "f32split":
+        # untimed: the diagnostic build's per-phase cycle counters
+        ctx.profile_enable(True)
+        ctx.profile_read()
+        ctx.phase_read()
+        for _ in range(2):
+            step(args.precision)
+        ctx.profile_read()
+        phases = phase_shares(ctx.phase_read())
+        ctx.profile_enable(False)
+
     # -------------------------------------------------------- CPU baseline
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -707,6 +741,8 @@ def main():
             line["graph_sweep"] = graph_info
         if tree:
             line["tree"] = tree
+        if phases:
+            line["phases"] = phases
         line.update(extras)
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -53,7 +53,8 @@ enum {
     SPHGRAV_ERR_OUT_OF_MEMORY = 5,
     SPHGRAV_ERR_PROTOCOL = 6,          /* lasthalf without firsthalf, and similar */
     SPHGRAV_ERR_DEVICE_TIMEOUT = 7,    /* a bounded device-side wait gave up */
-    SPHGRAV_ERR_TOO_LARGE = 8          /* size beyond a documented limit */
+    SPHGRAV_ERR_TOO_LARGE = 8,         /* size beyond a documented limit */
+    SPHGRAV_ERR_UNSUPPORTED = 9        /* feature not built into this library */
 };
 
 enum { SPHGRAV_FP64 = 0, SPHGRAV_F32SPLIT = 1, SPHGRAV_TREE = 2 };
@@ -292,6 +293,17 @@ int sphgrav_last_plan_info(sphgrav_ctx *ctx, int *nitems, int *nchunks_max,
  * count since the previous read (it synchronises the stream). */
 int sphgrav_profile_enable(sphgrav_ctx *ctx, int on);
 int sphgrav_profile_read(sphgrav_ctx *ctx, double *kernel_ms, int *launches);
+/* Phase accounting of the split-FP32 pair kernel, a diagnostic build
+ * (`python -m starsmasher_b200.build --phases` compiles the kernel with
+ * -DSG_PHASES into libsphgrav_b200_phases.so; the default library returns
+ * SPHGRAV_ERR_UNSUPPORTED).  While sphgrav_profile_enable is on, every
+ * split-FP32 launch adds the SM cycles its warps spend per phase; this call
+ * synchronises the stream, copies the 16 counters and zeroes them.  Order:
+ * consumer item fetch + barrier, row loads, waits for a staged tile, far loop,
+ * checked loop, FP64 near pairs, item end; producer waits, producer work;
+ * then counts of far and checked (warp, tile) pairs, near_eval calls and
+ * items per consumer warp.  No counterpart in the reference. */
+int sphgrav_phase_read(sphgrav_ctx *ctx, unsigned long long *counters, int n);
 /* FP32 FMA throughput probe: runs a packed-FMA loop for about `iters`
  * iterations per thread on the context's device and returns the measured
  * TFLOP/s (2 flops per FMA) in *tflops. */

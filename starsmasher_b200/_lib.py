@@ -9,7 +9,11 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsphgrav_b200.so")
+# SPHGRAV_B200_BUILD=phases loads the diagnostic build whose split-FP32 kernel
+# counts cycles per phase (`python -m starsmasher_b200.build --phases`)
+_BUILDS = {"": "libsphgrav_b200.so", "default": "libsphgrav_b200.so",
+           "phases": "libsphgrav_b200_phases.so"}
+LIB_PATH = os.path.join(HERE, _BUILDS[os.environ.get("SPHGRAV_B200_BUILD", "")])
 
 OK = 0
 ERR_INVALID_ARGUMENT = 1
@@ -20,6 +24,7 @@ ERR_OUT_OF_MEMORY = 5
 ERR_PROTOCOL = 6
 ERR_DEVICE_TIMEOUT = 7
 ERR_TOO_LARGE = 8
+ERR_UNSUPPORTED = 9
 
 FP64 = 0
 F32SPLIT = 1
@@ -78,6 +83,7 @@ SIGNATURES = {
     "sphgrav_forces_fp64_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "sphgrav_profile_enable": (_I, [_P, _I]),
     "sphgrav_profile_read": (_I, [_P, _PD, _PI]),
+    "sphgrav_phase_read": (_I, [_P, ctypes.POINTER(ctypes.c_ulonglong), _I]),
 }
 
 _lib = None

@@ -300,6 +300,17 @@ class Context:
               "sphgrav_profile_read")
         return ms.value, n.value
 
+    PHASES = ("item", "rows", "wait_full", "far", "checked", "near", "end",
+              "producer_wait", "producer_work", "n_far", "n_checked", "n_near", "n_items")
+
+    def phase_read(self) -> dict:
+        """Split-FP32 phase cycles summed over warps since the last read (the
+        diagnostic build only; the default build raises SphgravError with
+        status ERR_UNSUPPORTED).  Counted while profiling is enabled."""
+        buf = (ctypes.c_ulonglong * 16)()
+        check(self._lib.sphgrav_phase_read(self._h, buf, 16), "sphgrav_phase_read")
+        return {k: int(buf[i]) for i, k in enumerate(self.PHASES)}
+
     def fp32_peak_probe(self, iters: int = 20000) -> float:
         t = ctypes.c_double()
         check(self._lib.sphgrav_fp32_peak_probe(self._h, int(iters), ctypes.byref(t)),

@@ -7,6 +7,10 @@ Outputs (next to this file):
                          -lstdc++), so the Fortran host relinks unchanged.
 
 Every object is compiled for sm_100a only.  Usage: ``python -m starsmasher_b200.build``.
+
+``--phases`` also builds libsphgrav_b200_phases.so, a diagnostic copy whose
+split-FP32 kernel is compiled with -DSG_PHASES: its warps count SM cycles per
+phase (sphgrav_phase_read); load it with SPHGRAV_B200_BUILD=phases.
 """
 from __future__ import annotations
 
@@ -23,6 +27,7 @@ OBJDIR = os.path.join(HERE, "_build")
 SOURCES = ["sg_prep.cu", "sg_f64.cu", "sg_f32.cu", "sg_refine.cu", "sg_tree.cu", "sg_api.cu",
            "sg_noalloc.cu"]
 SO_NAME = "libsphgrav_b200.so"
+PHASES_SO_NAME = "libsphgrav_b200_phases.so"
 A_NAME = "libSPHgrav.a"
 
 NVCC_FLAGS = [
@@ -41,11 +46,13 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _compile(src: str, verbose: bool) -> str:
-    obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
-    cmd = [nvcc(), *NVCC_FLAGS, "-I", CSRC, "-I", INCLUDE, "-c", os.path.join(CSRC, src), "-o", obj]
+def _compile(src: str, verbose: bool, extra=(), suffix: str = "") -> str:
+    stem = os.path.splitext(src)[0] + suffix
+    obj = os.path.join(OBJDIR, stem + ".o")
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", CSRC, "-I", INCLUDE, "-c", os.path.join(CSRC, src),
+           "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
-    log = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".ptxas.txt")
+    log = os.path.join(OBJDIR, stem + ".ptxas.txt")
     with open(log, "w") as f:
         f.write(res.stdout + res.stderr)
     if res.returncode != 0:
@@ -88,5 +95,31 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return so
 
 
+def build_phases(force: bool = False, verbose: bool = False) -> str:
+    """The diagnostic library: the default objects with sg_f32.cu compiled
+    with -DSG_PHASES."""
+    so = os.path.join(HERE, PHASES_SO_NAME)
+    if not force and not _stale(so):
+        return so
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = []
+    for src in SOURCES:
+        if src == "sg_f32.cu":
+            continue
+        obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+        objs.append(obj if os.path.exists(obj) and not _stale(obj) else _compile(src, verbose))
+    objs.append(_compile("sg_f32.cu", verbose, extra=("-DSG_PHASES",), suffix="_phases"))
+    tmp = so + ".tmp"
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs,
+           "-lcudart"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    os.replace(tmp, so)
+    return so
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    if "--phases" in sys.argv:
+        print(build_phases(force="--force" in sys.argv, verbose=True))

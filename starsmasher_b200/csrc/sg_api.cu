@@ -240,6 +240,8 @@ struct sphgrav_ctx {
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
+    // phase cycles of the split-FP32 kernel (diagnostic build only)
+    DBuf<unsigned long long> phases;
 };
 
 template <class T>
@@ -842,6 +844,13 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     const bool want_g = precision == SPHGRAV_F32SPLIT && (refine || c->keep_scale);
     a.gpart = want_g ? c->gpart.p : nullptr;
     const bool timed = c->profiling && !c->capturing && P.nitems > 0;
+    if (timed && precision == SPHGRAV_F32SPLIT && phases_built()) {
+        if (!c->phases.p) {
+            TRY(ensure(c, c->phases, PHASE_COUNTERS, "phase counters"));
+            CUDA_TRY(cudaMemsetAsync(c->phases.p, 0, sizeof(unsigned long long) * PHASE_COUNTERS, st));
+        }
+        a.phases = c->phases.p;
+    }
     if (timed) {
         if (c->prof_used == c->prof_events.size()) {
             cudaEvent_t e0, e1;
@@ -1030,6 +1039,7 @@ const char *sphgrav_status_string(int s)
     case SPHGRAV_ERR_PROTOCOL: return "call protocol violated";
     case SPHGRAV_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
     case SPHGRAV_ERR_TOO_LARGE: return "size beyond a documented limit";
+    case SPHGRAV_ERR_UNSUPPORTED: return "not built into this library";
     default: return "unknown status";
     }
 }
@@ -1107,7 +1117,7 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->range2.release();
     c->gpart.release(); c->rcount.release(); c->rlist.release(); c->rnitems.release();
     c->rhead.release(); c->rsets.release(); c->ritems.release(); c->rpart.release();
-    c->scale.release();
+    c->scale.release(); c->phases.release();
     c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release();
     c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();
     c->twsum.release(); c->tgcount.release(); c->tgflag.release(); c->tglist.release();
@@ -1592,6 +1602,25 @@ int sphgrav_profile_read(sphgrav_ctx *c, double *kernel_ms, int *launches)
     if (kernel_ms) *kernel_ms = total;
     if (launches) *launches = (int)c->prof_used;
     c->prof_used = 0;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_phase_read(sphgrav_ctx *c, unsigned long long *counters, int n)
+{
+    if (!c || !counters || n < (int)PHASE_COUNTERS)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "need room for %d counters", (int)PHASE_COUNTERS);
+    if (!phases_built())
+        return set_err(SPHGRAV_ERR_UNSUPPORTED,
+                       "phase accounting needs the library built with -DSG_PHASES "
+                       "(python -m starsmasher_b200.build --phases)");
+    TRY(use_device(c));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < (int)PHASE_COUNTERS; i++) counters[i] = 0ull;
+    if (c->phases.p) {
+        CUDA_TRY(cudaMemcpy(counters, c->phases.p, sizeof(unsigned long long) * PHASE_COUNTERS,
+                            cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemset(c->phases.p, 0, sizeof(unsigned long long) * PHASE_COUNTERS));
+    }
     return SPHGRAV_OK;
 }
 

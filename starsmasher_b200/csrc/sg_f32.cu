@@ -278,6 +278,27 @@ struct WsSmem {
 // the rows of the benchmark workloads lie beyond 8 H).
 constexpr float SHIFT_H = 8.f;
 
+// Phase accounting (diagnostic build, -DSG_PHASES): every warp reads clock64
+// at its phase boundaries and lane 0 adds the elapsed cycles into a shared
+// per-warp row, flushed to ComputeArgs::phases when the CTA leaves.
+#ifdef SG_PHASES
+bool phases_built() { return true; }
+#define PH_MARK(i)                                                              \
+    do {                                                                        \
+        const long long t_ = clock64();                                         \
+        if (lane == 0) s_ph[warp][(i)] += (unsigned long long)(t_ - ph_t);      \
+        ph_t = t_;                                                              \
+    } while (0)
+#define PH_COUNT(i)                                 \
+    do {                                            \
+        if (lane == 0) s_ph[warp][(i)] += 1ull;     \
+    } while (0)
+#else
+bool phases_built() { return false; }
+#define PH_MARK(i) do {} while (0)
+#define PH_COUNT(i) do {} while (0)
+#endif
+
 template <int W, int K, int Q, int TJ, int NS, bool NEWTON, int FQ>
 __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 {
@@ -318,6 +339,10 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     const SortedF64 D = a.D;
     const SortedF32 F = a.F;
     const int nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
+#ifdef SG_PHASES
+    __shared__ unsigned long long s_ph[W + 1][PHASE_COUNTERS];
+    for (int i = tid; i < (W + 1) * PHASE_COUNTERS; i += NT) (&s_ph[0][0])[i] = 0ull;
+#endif
 
     if (tid == 0) {
         for (int s = 0; s < NS; s++) {
@@ -328,6 +353,9 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
         fence_mbar_init();
     }
     __syncthreads();
+#ifdef SG_PHASES
+    long long ph_t = clock64();
+#endif
 
     uint32_t g = 0;                        // tiles this CTA has passed through its ring
     bool failed = false;
@@ -367,6 +395,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
         const SetDesc S = a.sets[Wk.set];
         const ITileMeta C = a.imeta[S.tile_off + Wk.tile];
         const int ntile = (Wk.je - Wk.jb) / TJ;
+        PH_MARK(producer ? PH_PROD_WAIT : PH_ITEM);
 
         if (producer) {
             // ------------------------------------------------ producer warp
@@ -374,12 +403,14 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
             // consumers released tile gt - NS: wait for that before each bulk copy.
             if (ntile > 0) {
                 const bool ok = mbar_wait_bounded(&bar_empty[g % NS], ((g / NS) & 1) ^ 1, WAIT_LIMIT);
+                PH_MARK(PH_PROD_WAIT);
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(a.err, DEVERR_TIMEOUT);
                     failed = true;
                 } else if (lane == 0) {
                     issue(S, Wk.jb, g);
                 }
+                PH_MARK(PH_PROD_WORK);
             }
             for (int t = 0; t < ntile && !failed; t++) {
                 const uint32_t gt = g + t;
@@ -388,9 +419,12 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                 if (t + 1 < ntile) {
                     const uint32_t gn = gt + 1;
                     ok = mbar_wait_bounded(&bar_empty[gn % NS], ((gn / NS) & 1) ^ 1, WAIT_LIMIT);
+                    PH_MARK(PH_PROD_WAIT);
                     if (__all_sync(0xffffffffu, ok) && lane == 0) issue(S, Wk.jb + (t + 1) * TJ, gn);
+                    PH_MARK(PH_PROD_WORK);
                 }
                 ok = ok && mbar_wait_bounded(&bar_raw[s], (gt / NS) & 1, WAIT_LIMIT);
+                PH_MARK(PH_PROD_WAIT);
                 if (ok && lane == 0) pending[s] = false;
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(a.err, DEVERR_TIMEOUT);
@@ -437,6 +471,7 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                 }
                 __syncwarp();
                 mbar_arrive(&bar_full[s]);
+                PH_MARK(PH_PROD_WORK);
             }
         } else {
             // ----------------------------------------------- consumer warps
@@ -501,11 +536,14 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
             float slack[3];
 #pragma unroll
             for (int d = 0; d < 3; d++) slack[d] = 9.5367e-7f * fmaxf(fabsf(wlo[d]), fabsf(whi[d]));
+            PH_MARK(PH_ROWS);
+            PH_COUNT(PH_N_ITEMS);
 
             for (int t = 0; t < ntile; t++) {
                 const uint32_t gt = g + t;
                 const int s = gt % NS;
                 const bool ok = mbar_wait_bounded(&bar_full[s], (gt / NS) & 1, WAIT_LIMIT);
+                PH_MARK(PH_WAIT_FULL);
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(a.err, DEVERR_TIMEOUT);
                     failed = true;
@@ -630,6 +668,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                         fold(acc + 2 * NT, acc + 6 * NT, tz[k]);
                         fold(acc + 3 * NT, acc + 7 * NT, tp[k]);
                     }
+                    PH_MARK(far ? PH_FAR : PH_CHECKED);
+                    PH_COUNT(far ? PH_N_FAR : PH_N_CHECKED);
                     // deferred near-field pairs in FP64 (far is uniform over the warp)
                     if (!far && __any_sync(0xffffffffu, wsum != 0u)) {
                         unsigned char *cb = smem + L::COOP + warp * (L::COOP_RES + L::COOP_BUF);
@@ -638,6 +678,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                             s_row, s_acc, stage_raw(s),
                             reinterpret_cast<unsigned short *>(cb + L::COOP_RES),
                             reinterpret_cast<double *>(cb));
+                        PH_MARK(PH_NEAR);
+                        PH_COUNT(PH_N_NEAR);
                     }
                 }
                 mbar_arrive(&bar_empty[s]);
@@ -678,9 +720,14 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     }
                 }
             }
+            PH_MARK(PH_END);
         }
         g += ntile;
     }
+#ifdef SG_PHASES
+    if (a.phases && lane == 0)
+        for (int i = 0; i < PHASE_COUNTERS; i++) atomicAdd(a.phases + i, s_ph[warp][i]);
+#endif
     // never leave with bulk copies in flight into this CTA's shared memory
     if (producer && lane == 0) {
         for (int b = 0; b < NS; b++)

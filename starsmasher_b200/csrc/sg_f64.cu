@@ -43,13 +43,14 @@ __device__ __forceinline__ double rsqrt_f64(double r2)
 
 // Resident blocks per SM the register budget is sized for: 64K registers /
 // (NT * MINB) per thread (K = 1: 128, K = 2: 170, K >= 3: 255 at NT = 128).
-template <int NT, int K>
+// MB > 0 overrides the count.
+template <int NT, int K, int MB>
 struct F64Occ {
-    static constexpr int MINB = (K >= 3 ? 2 : (K == 2 ? 3 : 4)) * 128 / NT;
+    static constexpr int MINB = MB > 0 ? MB : (K >= 3 ? 2 : (K == 2 ? 3 : 4)) * 128 / NT;
 };
 
-template <int NT, int K, int TJ, int NS, int U>
-__global__ void __launch_bounds__(NT, F64Occ<NT, K>::MINB) k_fp64(ComputeArgs a)
+template <int NT, int K, int TJ, int NS, int U, int MB>
+__global__ void __launch_bounds__(NT, F64Occ<NT, K, MB>::MINB) k_fp64(ComputeArgs a)
 {
     static_assert(TJ % META_J == 0, "j-tile must hold whole metadata records");
     constexpr int ITILE = NT * K;
@@ -271,22 +272,27 @@ __global__ void __launch_bounds__(NT, F64Occ<NT, K>::MINB) k_fp64(ComputeArgs a)
     }
 }
 
-// name, threads NT, rows per thread K, j-tile TJ, stages NS, far-loop unroll U.
+// name, threads NT, rows per thread K, j-tile TJ, stages NS, far-loop unroll U,
+// resident blocks per SM the registers are sized for MB (0: by K and NT).
 // Variant 0 (the smallest row tile) also recomputes the split-FP32 refine rows.
-#define SG_F64_VARIANTS(X)                             \
-    X(128, 1, 128, 3, 2, "fp64_nt128_k1_tj128")        \
-    X(128, 2, 128, 3, 2, "fp64_nt128_k2_tj128")        \
-    X(128, 4, 128, 3, 2, "fp64_nt128_k4_tj128")        \
-    X(256, 1, 128, 3, 2, "fp64_nt256_k1_tj128")        \
-    X(128, 2, 256, 3, 2, "fp64_nt128_k2_tj256")        \
-    X(128, 4, 256, 3, 2, "fp64_nt128_k4_tj256")        \
-    X(128, 2, 256, 3, 4, "fp64_nt128_k2_tj256_u4")     \
-    X(128, 3, 256, 3, 2, "fp64_nt128_k3_tj256")
+#define SG_F64_VARIANTS(X)                                   \
+    X(128, 1, 128, 3, 2, 0, "fp64_nt128_k1_tj128")           \
+    X(128, 2, 128, 3, 2, 0, "fp64_nt128_k2_tj128")           \
+    X(128, 4, 128, 3, 2, 0, "fp64_nt128_k4_tj128")           \
+    X(256, 1, 128, 3, 2, 0, "fp64_nt256_k1_tj128")           \
+    X(128, 2, 256, 3, 2, 0, "fp64_nt128_k2_tj256")           \
+    X(128, 4, 256, 3, 2, 0, "fp64_nt128_k4_tj256")           \
+    X(128, 2, 256, 3, 4, 0, "fp64_nt128_k2_tj256_u4")        \
+    X(128, 3, 256, 3, 2, 0, "fp64_nt128_k3_tj256")           \
+    X(64, 2, 256, 3, 2, 0, "fp64_nt64_k2_tj256")             \
+    X(32, 2, 128, 3, 2, 0, "fp64_nt32_k2_tj128")             \
+    X(128, 2, 256, 3, 1, 4, "fp64_nt128_k2_tj256_u1_b4")     \
+    X(64, 3, 256, 3, 2, 0, "fp64_nt64_k3_tj256")
 
-#define SG_INFO(NT, K, TJ, NS, U, NAME) {0, NT, K, 1, TJ, 0, NAME, NT * K},
+#define SG_INFO(NT, K, TJ, NS, U, MB, NAME) {0, NT, K, 1, TJ, 0, NAME, NT * K},
 static const VariantInfo kF64Variants[] = {SG_F64_VARIANTS(SG_INFO)};
 #undef SG_INFO
-#define SG_PTR(NT, K, TJ, NS, U, NAME) (const void *)k_fp64<NT, K, TJ, NS, U>,
+#define SG_PTR(NT, K, TJ, NS, U, MB, NAME) (const void *)k_fp64<NT, K, TJ, NS, U, MB>,
 static const void *kF64Kernels[] = {SG_F64_VARIANTS(SG_PTR)};
 #undef SG_PTR
 constexpr int kNF64 = sizeof(kF64Variants) / sizeof(kF64Variants[0]);
@@ -298,9 +304,9 @@ const void *f64_kernel(int v) { return kF64Kernels[v]; }
 cudaError_t launch_f64(int v, int grid, const ComputeArgs &a, cudaStream_t st)
 {
     int idx = 0;
-#define SG_CASE(NT, K, TJ, NS, U, NAME)                            \
+#define SG_CASE(NT, K, TJ, NS, U, MB, NAME)                        \
     if (v == idx) {                                                \
-        k_fp64<NT, K, TJ, NS, U><<<grid, NT, 0, st>>>(a);          \
+        k_fp64<NT, K, TJ, NS, U, MB><<<grid, NT, 0, st>>>(a);      \
         ++g_launches;                                              \
         return cudaGetLastError();                                 \
     }                                                              \

@@ -70,7 +70,31 @@ struct ComputeArgs {
     int nkernel;
     int itile;
     float band2;         // split-FP32: pairs with r^2 < band2 * max(H^2) use FP64 (>= 1)
+    // split-FP32 built with -DSG_PHASES: [PHASE_COUNTERS] clock64 cycles per
+    // phase summed over warps (see the Phase enum); nullptr = not counted
+    unsigned long long *phases = nullptr;
 };
+
+// Phase accounting of the split-FP32 kernel (a diagnostic build: the pair
+// kernel compiled with -DSG_PHASES).  Consumer and producer warps sum the
+// SM cycles they spend in each phase; counts are per warp.
+enum Phase {
+    PH_ITEM = 0,      // consumer: queue fetch and the CTA barrier at an item start
+    PH_ROWS,          // consumer: loading the item's rows, warp box
+    PH_WAIT_FULL,     // consumer: waiting for a staged tile
+    PH_FAR,           // consumer: far loop + tile fold
+    PH_CHECKED,       // consumer: checked loop (near pairs masked) + tile fold
+    PH_NEAR,          // consumer: near_eval (FP64 pairs)
+    PH_END,           // consumer: combining and writing the item's partials
+    PH_PROD_WAIT,     // producer: waiting for a free stage or for its copies
+    PH_PROD_WORK,     // producer: issuing copies, rewriting tiles, tile boxes
+    PH_N_FAR,         // count: far (warp, tile) pairs
+    PH_N_CHECKED,     // count: checked (warp, tile) pairs
+    PH_N_NEAR,        // count: near_eval calls
+    PH_N_ITEMS,       // count: items started per consumer warp
+    PHASE_COUNTERS = 16
+};
+bool phases_built();
 
 struct VariantInfo {
     int precision;  // 0 fp64, 1 f32 split
