@@ -325,25 +325,34 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
         int v = variant_by_name(precision, it->second);
         if (v >= 0) return v;
     }
-    // FP64: two rows per thread and 256-source tiles from 2^18 on (262K:
-    // 804 vs 769 G pairs/s for one row per thread; 1M: 892 vs 831), one row
-    // and 128-source tiles below (16K: 224 vs 162; the batch of 4K-131K
-    // models: 725 vs 694)
-    if (precision == SPHGRAV_FP64) return b >= 18 ? 4 : 0;
-    // defaults by pair-weighted mean N = 2^b, from a sweep of single
-    // polytropes on B200 (G pairs/s of the chosen shape vs the runner-up):
-    //   b >= 20  W12K2Q1, 7 stages   (1M: 2027 vs 1942 for W15K1Q2)
-    //   18..19   W12K1Q1, 7 stages   (262K: 1745 vs 1714; 524K: 1937 vs 1920)
-    //   15..17   W15K1Q2             (32K-131K: 661-1448 vs 548-1410)
-    //   13..14   W12K1Q4, 7 stages   (8K: 178 vs 165; 16K: 370 vs 324)
-    //   <= 12    W8K1Q4              (4K: 75 vs 72)
+    const bool batch = offsets.size() > 2;
+    // FP64 (kernel ms on B200): one-warp CTAs with two rows per thread and
+    // 128-source tiles from 2^16 on, and for batches from 2^15 (64K: 6.40 vs
+    // 6.94 for one row per thread; 131K: 22.2 vs 24.0; 262K: 83.8 vs 86.7 for
+    // two rows in 4-warp CTAs; 1M: 1253 vs 1253; the batch of 4K-131K models:
+    // 157 vs 170; the 16 collision snapshots: 1397 vs 1450), one row per
+    // thread and 128-source tiles below (8K: 0.74 vs 1.11; 16K: 1.04 vs 1.32;
+    // 32K: 2.33 vs 2.42).  One-warp CTAs wait only on their own warp at the
+    // per-tile stage release.
+    if (precision == SPHGRAV_FP64) return (b >= 16 || (batch && b >= 15)) ? 9 : 0;
+    // split-FP32 defaults by pair-weighted mean N = 2^b, from sweeps on B200
+    // (pair-kernel ms of the chosen shape vs the runner-up):
+    //   b >= 18  W12K2Q1, 7 stages   (1M: 491.6; 262K collision: 35.42 vs
+    //                                 35.40 for W12K1Q1; the 16 collision
+    //                                 snapshots, mean 317K: 562 vs 579)
+    //   17, and batches from 2^15: W12K1Q1, 7 stages (131K: 9.28 vs 9.65 for
+    //                                 W15K1Q2; the batch of 4K-131K models,
+    //                                 mean 61K: 64.7 vs 67.3)
+    //   15..16   W15K1Q2             (32K: 0.791 vs 0.827; 64K: 2.52 vs 2.58)
+    //   13..14   W12K1Q4, 7 stages   (8K: 0.135 vs 0.142; 16K: 0.299 vs 0.298)
+    //   <= 12    W8K1Q4              (4K: 75 vs 72 G pairs/s)
     // Twelve consumer warps put the same number of consumers on every SMSP;
     // all without the Newton step on rsqrt.approx: in FP32 the step's own
     // roundings cost more than it corrects (RMS error 3.2e-8 vs 3.7e-8 at
     // N=1M, 2.7e-8 vs 4.4e-8 at N=16K, max error equal or lower on every
     // workload) and it is 3 of 16 FMA-pipe lane-ops per pair.
-    if (b >= 20) return 0;
-    if (b >= 18) return 2;
+    if (b >= 18) return 0;
+    if (b >= 17 || (batch && b >= 15)) return 2;
     if (b >= 15) return 3;
     if (b >= 13) return 5;
     return 4;

@@ -314,6 +314,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
     constexpr int RPW = 32 / Q;            // row groups per warp
     constexpr int ITILE = NT * K / Q;      // rows per i-tile
     constexpr int NMETA = L::NMETA;
+    static_assert(NMETA >= 1 && NMETA <= 32 && (NMETA & (NMETA - 1)) == 0,
+                  "tile box reduction: one record per lane, a power of two");
     constexpr float SA = Scales<NEWTON>::acc, SP = Scales<NEWTON>::pot;
     constexpr uint32_t WAIT_LIMIT = 1u << 22;
     constexpr int NSB = L::NSB;
@@ -431,43 +433,70 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
                     failed = true;
                     break;
                 }
-                // rewrite the tile relative to the i-tile centre
-                const float *rbuf = stage_raw(s);
-                const int rb = s;
-                float *cx = comp + s * 5 * TJ;
-#pragma unroll 4
-                for (int j = lane; j < TJ; j += 32) {
-                    cx[j] = __fadd_rn(__fsub_rn(rbuf[j], C.chx), __fsub_rn(rbuf[TJ + j], C.clx));
-                    cx[TJ + j] = __fadd_rn(__fsub_rn(rbuf[2 * TJ + j], C.chy),
-                                           __fsub_rn(rbuf[3 * TJ + j], C.cly));
-                    cx[2 * TJ + j] = __fadd_rn(__fsub_rn(rbuf[4 * TJ + j], C.chz),
-                                               __fsub_rn(rbuf[5 * TJ + j], C.clz));
-                    cx[3 * TJ + j] = rbuf[6 * TJ + j];
-                    cx[4 * TJ + j] = a.band2 * rbuf[7 * TJ + j];  // (band H)^2
-                }
-                if (lane == 0) {
-                    TileBox B;
-                    B.empty = 1;
-                    B.h2max = 0.f;
-                    for (int d = 0; d < 3; d++) { B.lo[d] = INFINITY; B.hi[d] = -INFINITY; }
-                    const float c3[3] = {C.chx, C.chy, C.chz};
+                // rewrite the tile relative to the i-tile centre (four sources
+                // per lane and step, 16-byte shared-memory accesses)
+                const float4 *rb4 = reinterpret_cast<const float4 *>(stage_raw(s));
+                float4 *cx4 = reinterpret_cast<float4 *>(comp + s * 5 * TJ);
+                constexpr int T4 = TJ / 4;
+                auto rel = [](float4 h, float4 l, float ch, float cl) {
+                    return make_float4(__fadd_rn(__fsub_rn(h.x, ch), __fsub_rn(l.x, cl)),
+                                       __fadd_rn(__fsub_rn(h.y, ch), __fsub_rn(l.y, cl)),
+                                       __fadd_rn(__fsub_rn(h.z, ch), __fsub_rn(l.z, cl)),
+                                       __fadd_rn(__fsub_rn(h.w, ch), __fsub_rn(l.w, cl)));
+                };
 #pragma unroll
-                    for (int r = 0; r < NMETA; r++) {
-                        const JMeta M = s_meta[rb * NMETA + r];
-                        if (M.ex < 0.f) continue;
-                        B.empty = 0;
-                        const float mc[3] = {M.cx, M.cy, M.cz}, me[3] = {M.ex, M.ey, M.ez};
-                        for (int d = 0; d < 3; d++) {
-                            const float rc = mc[d] - c3[d];
-                            // rounding of the float centres and of the staged
-                            // coordinates: widen by 2^-20 of the magnitudes
-                            const float e = me[d] + 9.5367e-7f * (fabsf(mc[d]) + fabsf(c3[d]) + me[d]);
-                            B.lo[d] = fminf(B.lo[d], rc - e);
-                            B.hi[d] = fmaxf(B.hi[d], rc + e);
+                for (int j = lane; j < T4; j += 32) {
+                    cx4[j] = rel(rb4[j], rb4[T4 + j], C.chx, C.clx);
+                    cx4[T4 + j] = rel(rb4[2 * T4 + j], rb4[3 * T4 + j], C.chy, C.cly);
+                    cx4[2 * T4 + j] = rel(rb4[4 * T4 + j], rb4[5 * T4 + j], C.chz, C.clz);
+                    cx4[3 * T4 + j] = rb4[6 * T4 + j];
+                    const float4 h = rb4[7 * T4 + j];
+                    cx4[4 * T4 + j] = make_float4(a.band2 * h.x, a.band2 * h.y, a.band2 * h.z,
+                                                  a.band2 * h.w);  // (band H)^2
+                }
+                // the tile's box relative to the centre: one record per lane,
+                // then a min/max reduction over the NMETA lanes (exact, so
+                // independent of the order)
+                {
+                    float lo[3] = {INFINITY, INFINITY, INFINITY};
+                    float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+                    float h2m = 0.f;
+                    int empty = 1;
+                    if (lane < NMETA) {
+                        const JMeta M = s_meta[s * NMETA + lane];
+                        if (M.ex >= 0.f) {
+                            empty = 0;
+                            const float c3[3] = {C.chx, C.chy, C.chz};
+                            const float mc[3] = {M.cx, M.cy, M.cz}, me[3] = {M.ex, M.ey, M.ez};
+#pragma unroll
+                            for (int d = 0; d < 3; d++) {
+                                const float rc = mc[d] - c3[d];
+                                // rounding of the float centres and of the staged
+                                // coordinates: widen by 2^-20 of the magnitudes
+                                const float e = me[d] + 9.5367e-7f * (fabsf(mc[d]) + fabsf(c3[d]) + me[d]);
+                                lo[d] = rc - e;
+                                hi[d] = rc + e;
+                            }
+                            h2m = a.band2 * M.h2max * 1.000001f;
                         }
-                        B.h2max = fmaxf(B.h2max, a.band2 * M.h2max * 1.000001f);
                     }
-                    s_box[s] = B;
+#pragma unroll
+                    for (int o = 1; o < NMETA; o <<= 1) {
+#pragma unroll
+                        for (int d = 0; d < 3; d++) {
+                            lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                            hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                        }
+                        h2m = fmaxf(h2m, __shfl_xor_sync(0xffffffffu, h2m, o));
+                        empty &= __shfl_xor_sync(0xffffffffu, empty, o);
+                    }
+                    if (lane == 0) {
+                        TileBox B;
+                        B.empty = empty;
+                        B.h2max = h2m;
+                        for (int d = 0; d < 3; d++) { B.lo[d] = lo[d]; B.hi[d] = hi[d]; }
+                        s_box[s] = B;
+                    }
                 }
                 __syncwarp();
                 mbar_arrive(&bar_full[s]);
