@@ -337,12 +337,16 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     if (precision == SPHGRAV_FP64) return (b >= 16 || (batch && b >= 15)) ? 9 : 0;
     // split-FP32 defaults by pair-weighted mean N = 2^b, from sweeps on B200
     // (pair-kernel ms of the chosen shape vs the runner-up):
-    //   b >= 18  W12K2Q1, 7 stages   (1M: 491.6; 262K collision: 35.42 vs
-    //                                 35.40 for W12K1Q1; the 16 collision
-    //                                 snapshots, mean 317K: 562 vs 579)
-    //   17, and batches from 2^15: W12K1Q1, 7 stages (131K: 9.28 vs 9.65 for
-    //                                 W15K1Q2; the batch of 4K-131K models,
-    //                                 mean 61K: 64.7 vs 67.3)
+    //   b >= 20, and batches from 2^18: W12K2Q1, 7 stages (1M: 488.5; the
+    //                                 16 collision snapshots, mean 317K: 562
+    //                                 vs 579 for W12K1Q1, whole call 587 vs 595)
+    //   17..19, and batches from 2^15: W12K1Q1, 7 stages (131K: 9.28 vs 9.65
+    //                                 for W15K1Q2; the batch of 4K-131K models,
+    //                                 mean 61K: 64.7 vs 67.3; 262K collision:
+    //                                 35.40 vs 35.42 for W12K2Q1, whose
+    //                                 768-row tiles leave more rows beyond
+    //                                 8 H of their centre for the FP64
+    //                                 refine: 2,357 rows, whole call 37.5 ms)
     //   15..16   W15K1Q2             (32K: 0.791 vs 0.827; 64K: 2.52 vs 2.58)
     //   13..14   W12K1Q4, 7 stages   (8K: 0.135 vs 0.142; 16K: 0.299 vs 0.298)
     //   <= 12    W8K1Q4              (4K: 75 vs 72 G pairs/s)
@@ -351,7 +355,7 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     // roundings cost more than it corrects (RMS error 3.2e-8 vs 3.7e-8 at
     // N=1M, 2.7e-8 vs 4.4e-8 at N=16K, max error equal or lower on every
     // workload) and it is 3 of 16 FMA-pipe lane-ops per pair.
-    if (b >= 18) return 0;
+    if (b >= 20 || (batch && b >= 18)) return 0;
     if (b >= 17 || (batch && b >= 15)) return 2;
     if (b >= 15) return 3;
     if (b >= 13) return 5;
