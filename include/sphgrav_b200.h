@@ -30,7 +30,13 @@
  *                      opening angle theta (sphgrav_set_theta, or
  *                      gpu_init_dev_'s theta for the legacy entry points;
  *                      default 0.3), softened pairs particle by particle.
- *                      One particle set per call; not capturable.
+ *                      Batches build one root per set (sets never interact).
+ *                      Eager calls read the tree's level table and group
+ *                      counts back to the host; inside a graph capture every
+ *                      count stays on the device (capture after an eager call
+ *                      of the same sizes, whose tree sizes the node array with
+ *                      2x headroom; a replay whose tree outgrows it reports
+ *                      SPHGRAV_ERR_TOO_LARGE at the next sphgrav_sync).
  *
  * Threading: a context is used by one host thread at a time.  Calls enqueue
  * work on the context's stream; functions that return results to host
@@ -200,6 +206,9 @@ int sphgrav_capture_end(sphgrav_ctx *ctx, sphgrav_graph **graph);
 int sphgrav_graph_launch(sphgrav_graph *graph, int repeats);
 /* 1 while the graph may be replayed (see above), else 0. */
 int sphgrav_graph_valid(const sphgrav_graph *graph);
+/* Releases a graph.  Called while this thread captures (a garbage-collected
+ * handle, say), the release waits until the capture ends: destroying a CUDA
+ * graph is not allowed during a capture and would invalidate it. */
 int sphgrav_graph_destroy(sphgrav_graph *graph);
 
 /* ------------------------------------------------------------ tuning --- */
@@ -250,6 +259,7 @@ int sphgrav_set_theta(sphgrav_ctx *ctx, double theta);
 /* SPHGRAV_TREE: walking groups of the last tree call and how many of them
  * were handed to the direct FP64 sum (groups with more than 8,192 particles
  * within the largest H of their box; their rows are exact direct sums).
+ * Both are -1 after a captured call (its counts stay on the device).
  * Either pointer may be NULL. */
 int sphgrav_tree_stats(sphgrav_ctx *ctx, int *groups, int *heavy);
 /* Force a kernel variant by index (-1 = automatic) for a precision. */

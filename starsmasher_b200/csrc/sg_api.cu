@@ -218,6 +218,7 @@ struct sphgrav_ctx {
     DBuf<double> theavy_part, tacc;
     DBuf<unsigned char> tgflag;
     DBuf<int2> tglist, tgorder;
+    DBuf<unsigned long long> tkeys;  // Hilbert keys by sorted slot (batches)
     DBuf<unsigned char> tscan;
     DBuf<double> tres, twsum;
     DBuf<float> probe_sink;
@@ -637,17 +638,19 @@ static SortedF32 sorted32(sphgrav_ctx *c)
 static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
                     int ni, const InputsDev &in, const OutputsDev &out, double *W, int nkernel)
 {
-    if (offsets.size() != 2)
-        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "the tree mode takes one particle set per call");
-    if (c->capturing)
-        return set_err(SPHGRAV_ERR_PROTOCOL,
-                       "the tree mode cannot be captured: its build reads the level table and "
-                       "the group counts back to the host");
     TRY(prepare(c, offsets, full_rows, i_lo, ni, SPHGRAV_FP64, 0));
     const Plan &P = c->plan;
     cudaStream_t st = c->stream;
-    const int n = P.ntot;
-    if (n == 0) return SPHGRAV_OK;
+    const int n = P.ntot, nslots = P.npad_tot, nsets = P.nsets;
+    if (n == 0) {
+        if (W && nsets > 0) CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * nsets, st));
+        return SPHGRAV_OK;
+    }
+    // Inside a graph capture every count stays on the device: all key levels
+    // are issued, grids are sized for bounds and kernels read the counts
+    // there; buffers must already have the sizes an eager call of the same
+    // sizes gave them (ensure refuses to grow during a capture).
+    const bool dev = c->capturing;
     SortedF64 D = sorted64(c);
     SortedF32 F = sorted32(c);
     CUDA_TRY(launch_validate(in, n, c->err.p, st));
@@ -657,75 +660,116 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     CUDA_TRY(launch_sort(c->sort_temp.p, c->sort_temp.cap, c->keys_in.p, c->keys_out.p,
                          c->vals_in.p, c->vals_out.p, n, P.end_bit, st));
     CUDA_TRY(launch_gather(c->sets.p, P.nsets, P.max_npad, in, c->vals_out.p, D, F, st));
+    // the tree indexes sorted slots; with one set they are the sorted order
+    const unsigned long long *keys = c->keys_out.p;
+    if (nsets > 1) {
+        TRY(ensure(c, c->tkeys, (size_t)nslots, "tree keys"));
+        CUDA_TRY(tree_slot_keys(c->sets.p, nsets, P.max_n, c->keys_out.p, c->tkeys.p, st));
+        keys = c->tkeys.p;
+    }
     TRY(ensure(c, c->tcnt, (size_t)n + 1, "tree scratch"));
     TRY(ensure(c, c->toff, (size_t)n + 1, "tree scratch"));
-    TRY(ensure(c, c->tscan, tree_scan_temp_bytes(n + 1), "tree scan"));
-    TRY(ensure(c, c->tnodes, std::max<size_t>(c->tnodes.cap, 2 * (size_t)n + 64), "tree nodes"));
+    // scan scratch, also for a walking-order sort of up to n groups (the
+    // bound a captured call sorts)
+    TRY(ensure(c, c->tscan, std::max(tree_scan_temp_bytes(n + 1), tree_order_temp_bytes(n)),
+               "tree scan"));
+    TRY(ensure(c, c->tnodes, std::max<size_t>(c->tnodes.cap, 2 * (size_t)n + 64 + nsets), "tree nodes"));
     // walking groups: runs of sibling nodes with <= TREE_GROUP particles
     TRY(ensure(c, c->tglist, (size_t)n, "tree groups"));
+    TRY(ensure(c, c->tgorder, (size_t)n, "tree groups"));
+    TRY(ensure(c, c->theavy, (size_t)n, "tree heavy groups"));
     TRY(ensure(c, c->tgcount, 2, "tree groups"));  // [0] groups, [1] heavy groups
     TRY(ensure(c, c->tlv, TREE_LV_SIZE, "tree levels"));
-    // The build is issued TREE_BATCH levels at a time; one read-back of the
-    // level table per batch shows whether the tree has ended (an empty level)
-    // or the node array is full (it is regrown and the build repeated).
-    constexpr int TREE_BATCH = 4;
+    const int levels = P.bits;
+    TreeBuildArgs t;
+    t.n = n;
+    t.levels = levels;
+    t.nroots = nsets;
+    t.sets = c->sets.p;
+    t.keys = keys;
+    t.cnt = c->tcnt.p;
+    t.off = c->toff.p;
+    t.scan_temp = c->tscan.p;
+    t.scan_temp_bytes = c->tscan.cap;
+    t.lv = c->tlv.p;
     int lvh[TREE_LV_SIZE];
-    int nn = 0, depth = 0;
-    for (;;) {
-        TRY(ensure(c, c->tgflag, c->tnodes.cap, "tree groups"));
-        TreeBuildArgs t;
-        t.n = n;
-        t.keys = c->keys_out.p;
-        t.nodes = c->tnodes.p;
-        t.cap = (int)std::min<size_t>(c->tnodes.cap, 0x7fffffff);
-        t.cnt = c->tcnt.p;
-        t.off = c->toff.p;
-        t.scan_temp = c->tscan.p;
-        t.scan_temp_bytes = c->tscan.cap;
-        t.gflag = c->tgflag.p;
-        t.lv = c->tlv.p;
-        bool overflow = false;
-        for (int l0 = 0; l0 < TREE_LEVELS; l0 += TREE_BATCH) {
-            const int l1 = std::min(l0 + TREE_BATCH, TREE_LEVELS);
-            CUDA_TRY(tree_build_levels(t, l0, l1, st));
-            CUDA_TRY(cudaMemcpyAsync(lvh, c->tlv.p, sizeof(lvh), cudaMemcpyDeviceToHost, st));
-            CUDA_TRY(cudaStreamSynchronize(st));
-            overflow = lvh[TREE_LV_OVERFLOW] != 0;
-            nn = lvh[l1 + 1];  // end of level l1, the last one written
-            depth = l1;
-            if (overflow || lvh[l1 + 1] == lvh[l1]) break;  // level l1 is empty
+    DevCount nn{0, nullptr};
+    int depth = 0;
+    if (!dev) {
+        // Eager: TREE_BATCH levels at a time; one read-back of the level
+        // table per batch shows whether the tree has ended (an empty level)
+        // or the node array is full (it is regrown and the build repeated).
+        constexpr int TREE_BATCH = 4;
+        for (;;) {
+            TRY(ensure(c, c->tgflag, c->tnodes.cap, "tree groups"));
+            t.nodes = c->tnodes.p;
+            t.cap = (int)std::min<size_t>(c->tnodes.cap, 0x7fffffff);
+            t.gflag = c->tgflag.p;
+            bool overflow = false;
+            for (int l0 = 0; l0 < levels; l0 += TREE_BATCH) {
+                const int l1 = std::min(l0 + TREE_BATCH, levels);
+                CUDA_TRY(tree_build_levels(t, l0, l1, st));
+                CUDA_TRY(cudaMemcpyAsync(lvh, c->tlv.p, sizeof(lvh), cudaMemcpyDeviceToHost, st));
+                CUDA_TRY(cudaStreamSynchronize(st));
+                overflow = lvh[TREE_LV_OVERFLOW] != 0;
+                nn.host = lvh[l1 + 1];  // end of level l1, the last one written
+                depth = l1;
+                if (overflow || lvh[l1 + 1] == lvh[l1]) break;  // level l1 is empty
+            }
+            if (!overflow) break;
+            TRY(ensure(c, c->tnodes, 2 * c->tnodes.cap, "tree nodes"));
         }
-        if (!overflow) break;
-        TRY(ensure(c, c->tnodes, 2 * c->tnodes.cap, "tree nodes"));
+        while (depth > 0 && lvh[depth + 1] == lvh[depth]) depth--;  // deepest non-empty level
+        // room for a captured call of these sizes: twice this tree's nodes
+        const size_t room = std::min<size_t>(c->tnodes.cap, 2 * (size_t)nn.host + 1024);
+        TRY(ensure(c, c->tgeom, room, "tree geometry"));
+        TRY(ensure(c, c->tmp, room, "tree multipoles"));
+        TRY(ensure(c, c->tacc, tree_acc_bytes((int)room) / sizeof(double), "tree node sums"));
+    } else {
+        // Captured: every level, no read-back; the node capacity is what the
+        // eager call left (twice its tree); a replay whose tree needs more
+        // raises DEVERR_TREE_CAP (SPHGRAV_ERR_TOO_LARGE at the next sync)
+        const size_t cap = std::min({c->tnodes.cap, c->tgflag.cap, c->tgeom.cap, c->tmp.cap,
+                                     c->tacc.cap * sizeof(double) / tree_acc_bytes(1)});
+        if (cap < (size_t)nsets + 1 || !c->tgflag.p || !c->tgeom.p)
+            return set_err(SPHGRAV_ERR_PROTOCOL,
+                           "capture a tree call only after an eager tree call of the same sizes");
+        t.nodes = c->tnodes.p;
+        t.cap = (int)std::min<size_t>(cap, 0x7fffffff);
+        t.gflag = c->tgflag.p;
+        CUDA_TRY(tree_build_levels(t, 0, levels, st));
+        CUDA_TRY(tree_check_build(c->tlv.p, c->err.p, st));
+        nn = DevCount{t.cap, c->tlv.p + levels + 1};
+        depth = levels;
     }
-    while (depth > 0 && lvh[depth + 1] == lvh[depth]) depth--;  // deepest non-empty level
     CUDA_TRY(tree_groups(nn, c->tnodes.p, c->tgflag.p, c->tglist.p, c->tgcount.p, st));
-    int ngroups = 0;
-    CUDA_TRY(cudaMemcpyAsync(&ngroups, c->tgcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    const int *level_start = lvh;
+    DevCount ng{n, c->tgcount.p};
+    if (!dev) {
+        CUDA_TRY(cudaMemcpyAsync(&ng.host, c->tgcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        ng.dev = nullptr;
+    }
     // walking order: largest H first (the build's scratch holds the sort keys)
-    TRY(ensure(c, c->tgorder, (size_t)std::max(ngroups, 1), "tree groups"));
-    TRY(ensure(c, c->tscan, tree_order_temp_bytes(ngroups), "tree scan"));
-    CUDA_TRY(tree_order_groups(ngroups, c->tglist.p, c->tgorder.p, D.h2, (unsigned *)c->tcnt.p,
+    CUDA_TRY(tree_order_groups(ng, c->tglist.p, c->tgorder.p, D.h2, (unsigned *)c->tcnt.p,
                                (unsigned *)c->toff.p, c->tscan.p, c->tscan.cap, st));
-    TRY(ensure(c, c->tgeom, (size_t)nn, "tree geometry"));
-    TRY(ensure(c, c->tmp, (size_t)nn, "tree multipoles"));
-    TRY(ensure(c, c->tacc, tree_acc_bytes(nn) / sizeof(double), "tree node sums"));
-    CUDA_TRY(tree_props(nn, c->tnodes.p, D, c->theta, level_start, depth, c->tacc.p, c->tgeom.p,
-                        c->tmp.p, st));
+    CUDA_TRY(tree_props(nn, c->tnodes.p, D, c->theta, c->tlv.p, dev ? nullptr : lvh, depth, n,
+                        c->tacc.p, c->tgeom.p, c->tmp.p, st));
     TRY(ensure(c, c->tstack, (size_t)tree_walk_warps(c->sm_count) * TREE_STACK, "tree stack"));
-    TRY(ensure(c, c->tres, 4 * (size_t)n, "tree results"));
+    TRY(ensure(c, c->tres, 4 * (size_t)nslots, "tree results"));
+    // heavy groups' partial sums: room for TREE_HEAVY_CAP groups (a captured
+    // call's bound), more when an eager call finds more
+    TRY(ensure(c, c->theavy_part, tree_heavy_partials(TREE_HEAVY_CAP, P.max_n), "tree heavy sums"));
     CUDA_TRY(cudaMemsetAsync(c->head.p, 0, sizeof(int), st));
     TreeWalkArgs a;
     a.nodes = c->tnodes.p;
     a.geom = c->tgeom.p;
     a.mp = c->tmp.p;
     a.D = D;
-    a.n = n;
-    a.ngroups = ngroups;
+    a.n = nslots;
+    a.ngroups = ng.host;
+    a.ngroups_dev = ng.dev;
+    a.nroots = nsets;
     a.groups = c->tgorder.p;
-    TRY(ensure(c, c->theavy, (size_t)std::max(ngroups, 1), "tree heavy groups"));
     CUDA_TRY(cudaMemsetAsync(c->tgcount.p + 1, 0, sizeof(int), st));
     a.heavy = c->theavy.p;
     a.nheavy = c->tgcount.p + 1;
@@ -735,7 +779,7 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
     a.stack_cap = TREE_STACK;
     a.out = c->tres.p;
     a.err = c->err.p;
-    const bool timed = c->profiling;
+    const bool timed = c->profiling && !dev;
     if (timed) {
         if (c->prof_used == c->prof_events.size()) {
             cudaEvent_t e0, e1;
@@ -746,21 +790,27 @@ static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_r
         CUDA_TRY(cudaEventRecord(c->prof_events[c->prof_used].first, st));
     }
     CUDA_TRY(tree_walk(a, c->sm_count, st));
-    // groups whose particles' softening spheres hold too many particles: direct FP64
-    int nheavy = 0;
-    CUDA_TRY(cudaMemcpyAsync(&nheavy, c->tgcount.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    if (nheavy > 0) {
-        TRY(ensure(c, c->theavy_part, (size_t)nheavy * tree_heavy_chunks(nheavy, n) * 4 * 32,
-                   "tree heavy sums"));
-        CUDA_TRY(tree_heavy(nheavy, c->theavy.p, c->tgorder.p, D, n, nkernel, c->theavy_part.p,
-                            c->tres.p, st));
+    // groups whose particles' softening spheres hold too many particles: the
+    // direct FP64 sum over their own set
+    int nheavy = -1;
+    if (!dev) {
+        CUDA_TRY(cudaMemcpyAsync(&nheavy, c->tgcount.p + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        if (nheavy > TREE_HEAVY_CAP)
+            TRY(ensure(c, c->theavy_part, tree_heavy_partials(nheavy, P.max_n), "tree heavy sums"));
     }
-    c->tree_groups_last = ngroups;
+    if (dev || nheavy > 0) {
+        const int hcap = dev ? TREE_HEAVY_CAP : std::max(nheavy, TREE_HEAVY_CAP);
+        CUDA_TRY(tree_heavy(dev ? 0 : nheavy, c->tgcount.p + 1, hcap, c->theavy.p, c->tgorder.p,
+                            c->tnodes.p, nsets, D, nslots, P.max_n, nkernel, c->theavy_part.p,
+                            c->tres.p, c->err.p, st));
+    }
+    c->tree_groups_last = dev ? -1 : ng.host;
     c->tree_heavy_last = nheavy;
     if (timed) CUDA_TRY(cudaEventRecord(c->prof_events[c->prof_used++].second, st));
-    CUDA_TRY(tree_scatter(n, full_rows ? 0 : i_lo, full_rows ? n : ni, c->tres.p, D.orig, out, st));
-    if (W) CUDA_TRY(tree_wsum(n, c->tres.p, D.m, W, st));
+    CUDA_TRY(tree_scatter(nslots, full_rows ? 0 : i_lo, full_rows ? n : ni, c->tres.p, D.orig, out,
+                          st));
+    if (W) CUDA_TRY(tree_wsum(c->sets.p, nsets, nslots, c->tres.p, D.m, W, st));
     return SPHGRAV_OK;
 }
 
@@ -778,8 +828,7 @@ static int run_refine(sphgrav_ctx *c, int nkernel, const SortedF64 &D, const Out
                                 (int)std::min<size_t>(c->ritems.cap, 0x7fffffff), c->rsets.p,
                                 c->ritems.p, c->rnitems.p, c->err.p, st));
     CUDA_TRY(cudaMemsetAsync(c->rhead.p, 0, sizeof(int), st));
-    ComputeArgs a;
-    memset(&a, 0, sizeof(a));
+    ComputeArgs a{};
     a.sets = c->rsets.p;
     a.items = c->ritems.p;
     a.nitems = 0;
@@ -837,7 +886,7 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     // source boxes: both kernels skip the per-pair near test on far tiles
     CUDA_TRY(launch_jmeta(c->sets.p, P.nsets, P.nmeta, c->meta_set.p, D, c->jmeta.p, st));
     CUDA_TRY(cudaMemsetAsync(c->head.p, 0, sizeof(int), st));
-    ComputeArgs a;
+    ComputeArgs a{};
     a.sets = c->sets.p;
     a.items = c->items.p;
     a.nitems = P.nitems;
@@ -910,6 +959,10 @@ static int read_device_error(sphgrav_ctx *c)
     if (e & DEVERR_TIMEOUT) return set_err(SPHGRAV_ERR_DEVICE_TIMEOUT, "device wait timed out");
     if (e & DEVERR_TREE)
         return set_err(SPHGRAV_ERR_TOO_LARGE, "tree walk: traversal stack full (theta too small for N?)");
+    if (e & DEVERR_TREE_CAP)
+        return set_err(SPHGRAV_ERR_TOO_LARGE,
+                       "captured tree call: the tree outgrew the node array or the heavy-group "
+                       "list sized by the eager call before the capture; capture again");
     return SPHGRAV_OK;
 }
 
@@ -1131,7 +1184,7 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->gpart.release(); c->rcount.release(); c->rlist.release(); c->rnitems.release();
     c->rhead.release(); c->rsets.release(); c->ritems.release(); c->rpart.release();
     c->scale.release(); c->phases.release();
-    c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release();
+    c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release(); c->tkeys.release();
     c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();
     c->twsum.release(); c->tgcount.release(); c->tgflag.release(); c->tglist.release();
     c->tgorder.release(); c->tlv.release();
@@ -1292,6 +1345,8 @@ int sphgrav_lasthalf(sphgrav_ctx *c, double *ax, double *ay, double *az, double 
     if (e & DEVERR_TIMEOUT) return set_err(SPHGRAV_ERR_DEVICE_TIMEOUT, "device wait timed out");
     if (e & DEVERR_TREE)
         return set_err(SPHGRAV_ERR_TOO_LARGE, "tree walk: traversal stack full (theta too small for N?)");
+    if (e & DEVERR_TREE_CAP)
+        return set_err(SPHGRAV_ERR_TOO_LARGE, "tree: node array or heavy-group list full");
     const int ni = c->pend_ni, i0 = c->pend_i0;
     if (ni > 0 && (!ax || !ay || !az || !pot))
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL output pointer");
@@ -1363,6 +1418,20 @@ int sphgrav_kick_reset(sphgrav_ctx *c, unsigned long long v)
     return SPHGRAV_OK;
 }
 
+// Captures are thread-local: while this thread captures, destroying a graph
+// (an unsafe call during a capture, which would invalidate it) is deferred
+// until its last capture ends.  A garbage-collected graph handle from an
+// earlier capture is the usual case.
+static thread_local int t_captures = 0;
+static thread_local std::vector<sphgrav_graph *> t_deferred_graphs;
+
+static void destroy_graph_now(sphgrav_graph *G)
+{
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    delete G;
+}
+
 int sphgrav_capture_begin(sphgrav_ctx *c)
 {
     if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
@@ -1370,6 +1439,7 @@ int sphgrav_capture_begin(sphgrav_ctx *c)
     TRY(use_device(c));
     CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     c->capturing = true;
+    ++t_captures;
     return SPHGRAV_OK;
 }
 
@@ -1380,7 +1450,12 @@ int sphgrav_capture_end(sphgrav_ctx *c, sphgrav_graph **out)
     c->capturing = false;
     TRY(use_device(c));
     cudaGraph_t g = nullptr;
-    CUDA_TRY(cudaStreamEndCapture(c->stream, &g));
+    const cudaError_t ended = cudaStreamEndCapture(c->stream, &g);
+    if (--t_captures == 0) {  // no capture left on this thread: release deferred graphs
+        for (sphgrav_graph *D : t_deferred_graphs) destroy_graph_now(D);
+        t_deferred_graphs.clear();
+    }
+    CUDA_TRY(ended);
     sphgrav_graph *G = new sphgrav_graph();
     G->graph = g;
     G->stream = c->stream;
@@ -1422,9 +1497,12 @@ int sphgrav_graph_destroy(sphgrav_graph *G)
 {
     if (!G) return SPHGRAV_OK;
     if (G->ctx) G->ctx->graphs.erase(G);
-    if (G->exec) cudaGraphExecDestroy(G->exec);
-    if (G->graph) cudaGraphDestroy(G->graph);
-    delete G;
+    G->ctx = nullptr;
+    if (t_captures > 0) {
+        t_deferred_graphs.push_back(G);
+        return SPHGRAV_OK;
+    }
+    destroy_graph_now(G);
     return SPHGRAV_OK;
 }
 

@@ -67,6 +67,7 @@ enum : int {
     DEVERR_INPUT = 1,
     DEVERR_TIMEOUT = 2,
     DEVERR_TREE = 4,  // tree walk: traversal stack full
+    DEVERR_TREE_CAP = 8,  // captured tree call: node array or heavy-group list full
 };
 
 // Self-potential constants c of the zero-distance rule (cpu_grav.f:141,

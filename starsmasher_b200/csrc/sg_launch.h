@@ -174,9 +174,12 @@ constexpr int TREE_BUDGET = 8192;  // particles within the largest H of a group'
                                    // tested pair by pair) before the group is handed to the
                                    // direct FP64 sum; a typical group has ~500-800
 constexpr int TREE_HEAVY_CHUNKS = 1024;  // most source chunks of a heavy group's direct sum
+// Heavy groups a captured (device-counted) tree call can hand to the direct
+// sum; more set DEVERR_TREE_CAP.  Partial sums: (4096 + cap) chunks.
+constexpr int TREE_HEAVY_CAP = 4096;
 // Source chunks per heavy group: about 4096 blocks in all, at least 2048 sources
-// each, 1..TREE_HEAVY_CHUNKS.
-inline int tree_heavy_chunks(int nheavy, int n)
+// each, 1..TREE_HEAVY_CHUNKS (n: the largest set's particles).
+__host__ __device__ inline int tree_heavy_chunks(int nheavy, int n)
 {
     int c = (4096 + nheavy - 1) / (nheavy > 0 ? nheavy : 1);
     if (c > n / 2048) c = n / 2048;
@@ -202,8 +205,11 @@ struct NodeMP {        // multipoles (64 bytes)
     float pad_[2];
 };
 struct TreeBuildArgs {
-    int n;
-    const unsigned long long *keys;  // sorted Hilbert keys of the n particles
+    int n;                           // particles (all sets)
+    int levels;                      // key digits per set: bits per axis (<= TREE_LEVELS)
+    int nroots;                      // sets: level 0 holds one root per set
+    const SetDesc *sets;             // root s spans [sets[s].poff, sets[s].poff + sets[s].n)
+    const unsigned long long *keys;  // Hilbert keys by sorted slot (set index in the top bits)
     TreeNode *nodes;
     int cap;                         // node capacity
     int *cnt, *off;                  // per-level scratch (n + 1 entries)
@@ -217,7 +223,9 @@ struct TreeWalkArgs {
     const NodeGeom *geom;
     const NodeMP *mp;
     SortedF64 D;
-    int n, ngroups, nkernel;
+    int n, ngroups, nkernel;   // n: result stride (sorted slots, pads included)
+    const int *ngroups_dev;    // when non-null the group count is read here
+    int nroots;                // roots are nodes [0, nroots), one per set
     const int2 *groups;  // [ngroups] sorted-slot ranges (start, end), end - start <= 32
     int *head;       // group counter (zeroed before the launch)
     int *heavy;      // [ngroups] groups handed to the direct sum ...
@@ -228,32 +236,56 @@ struct TreeWalkArgs {
     int *err;
 };
 size_t tree_scan_temp_bytes(int n);
+// Slot-indexed keys of every set's particles (pads are in no node).
+cudaError_t tree_slot_keys(const SetDesc *sets, int nsets, int max_n,
+                           const unsigned long long *keys_sorted, unsigned long long *keys_slot,
+                           cudaStream_t st);
 // Octree build: issues levels [level_begin, level_end) without a host wait
 // (level 0 also sets up the root); t.lv receives the level table (nodes of
 // level l are [lv[l], lv[l + 1])) and a flag set when `cap` nodes do not
 // suffice (the caller regrows the node array and builds again).
 cudaError_t tree_build_levels(const TreeBuildArgs &t, int level_begin, int level_end,
                               cudaStream_t st);
+// Counts that the host either knows (eager calls: read back) or leaves on the
+// device (calls inside a graph capture): `dev` non-null means "read it there",
+// `host` then bounds it (grids are sized for the bound, kernels loop).
+struct DevCount {
+    int host;
+    const int *dev;
+    __device__ int get() const { return dev ? *dev : host; }
+};
 // Lists the walking groups (order not significant); *ngroups via `count`.
-cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag, int2 *glist,
-                        int *count, cudaStream_t st);
+cudaError_t tree_groups(DevCount nn, const TreeNode *nodes, const unsigned char *gflag,
+                        int2 *glist, int *count, cudaStream_t st);
 // Groups sorted by descending largest H^2 of their particles (walking order).
 size_t tree_order_temp_bytes(int ng);
-cudaError_t tree_order_groups(int ng, const int2 *glist, int2 *ordered, const double *h2,
+cudaError_t tree_order_groups(DevCount ng, const int2 *glist, int2 *ordered, const double *h2,
                               unsigned *keys_in, unsigned *keys_out, void *temp, size_t temp_bytes,
                               cudaStream_t st);
-// Node properties; acc_buf: tree_acc_bytes(nn) of scratch.
+// Node properties; acc_buf: tree_acc_bytes(nn) of scratch.  Levels
+// [0, depth) are combined bottom-up; their node ranges are read from the
+// device level table lv (level_start, when given, sizes the grids exactly).
 size_t tree_acc_bytes(int nn);
-cudaError_t tree_props(int nn, const TreeNode *nodes, const SortedF64 &D, double theta,
-                       const int *level_start, int depth, void *acc_buf, NodeGeom *geom,
-                       NodeMP *mp, cudaStream_t st);
+cudaError_t tree_props(DevCount nn, const TreeNode *nodes, const SortedF64 &D, double theta,
+                       const int *lv, const int *level_start, int depth, int level_bound,
+                       void *acc_buf, NodeGeom *geom, NodeMP *mp, cudaStream_t st);
 int tree_walk_warps(int sm_count);
 cudaError_t tree_walk(const TreeWalkArgs &a, int sm_count, cudaStream_t st);
-cudaError_t tree_scatter(int n, int i_lo, int ni, const double *res, const int *orig,
+cudaError_t tree_scatter(int nslots, int i_lo, int ni, const double *res, const int *orig,
                          const OutputsDev &out, cudaStream_t st);
-cudaError_t tree_wsum(int n, const double *res, const double *m, double *W, cudaStream_t st);
-// Direct FP64 sums (all n sources) for the groups the walk handed over.
-cudaError_t tree_heavy(int nheavy, const int *heavy, const int2 *groups, const SortedF64 &D, int n,
-                       int nkernel, double *partials, double *out, cudaStream_t st);
+// W of every set (one block per set, fixed order); res stride nslots.
+cudaError_t tree_wsum(const SetDesc *sets, int nsets, int nslots, const double *res,
+                      const double *m, double *W, cudaStream_t st);
+// Direct FP64 sums over the group's own set for the groups the walk handed
+// over (*nheavy on the device, at most `cap`; more set DEVERR_TREE_CAP).
+// max_n: the largest set; nheavy_host > 0 sizes the grid exactly.
+cudaError_t tree_heavy(int nheavy_host, const int *nheavy, int cap, const int *heavy,
+                       const int2 *groups, const TreeNode *nodes, int nroots, const SortedF64 &D,
+                       int nslots, int max_n, int nkernel, double *partials, double *out, int *err,
+                       cudaStream_t st);
+// Partial-sum doubles tree_heavy needs for up to `cap` heavy groups.
+size_t tree_heavy_partials(int cap, int max_n);
+// Raises DEVERR_TREE_CAP when the build ran out of nodes (lv overflow flag).
+cudaError_t tree_check_build(const int *lv, int *err, cudaStream_t st);
 
 }  // namespace sg

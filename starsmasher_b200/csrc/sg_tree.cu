@@ -55,12 +55,13 @@ __device__ __forceinline__ int lower_bound_key(const unsigned long long *keys, i
 }
 
 // Children of node i of level `level` (keys of its particles share their
-// top 3*level key bits): the eight 3-bit digits of level + 1 split its
-// sorted range; b[0..8] are the digit boundaries.
-__device__ __forceinline__ void child_bounds(const TreeNode &T, int level,
+// set index and top 3*level spatial key bits): the eight 3-bit digits of
+// level + 1 split its sorted range; b[0..8] are the digit boundaries.
+// `levels` = the keys' bits per axis (digits per set).
+__device__ __forceinline__ void child_bounds(const TreeNode &T, int level, int levels,
                                              const unsigned long long *keys, int b[9])
 {
-    const int sh = 3 * (TREE_LEVELS - 1 - level);  // digit of level + 1
+    const int sh = 3 * (levels - 1 - level);  // digit of level + 1
     const unsigned long long base = (keys[T.start] >> (sh + 3)) << (sh + 3);
     b[0] = T.start;
     b[8] = T.end;
@@ -71,10 +72,10 @@ __device__ __forceinline__ void child_bounds(const TreeNode &T, int level,
 // Level bounds live on the device (lv[L] = first node of level L, lv[L + 1]
 // its end; lv[TREE_LV_OVERFLOW] set when the node array is too small), so the
 // host issues every level without waiting.  Level L has at most `bound`
-// nodes (min(8^L, n)); counts are written for the whole bound, zero past the
-// level's end, so that one fixed-size scan gives the child offsets.
-__global__ void k_tree_count(int level, int bound, const int *lv, const TreeNode *nodes,
-                             const unsigned long long *keys, int *cnt)
+// nodes (min(roots 8^L, n)); counts are written for the whole bound, zero past
+// the level's end, so that one fixed-size scan gives the child offsets.
+__global__ void k_tree_count(int level, int levels, int bound, const int *lv,
+                             const TreeNode *nodes, const unsigned long long *keys, int *cnt)
 {
     const int l0 = lv[level], l1 = lv[level + 1];
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < bound; j += gridDim.x * blockDim.x) {
@@ -82,9 +83,9 @@ __global__ void k_tree_count(int level, int bound, const int *lv, const TreeNode
         int c = 0;
         if (i < l1) {
             const TreeNode T = nodes[i];
-            if (T.end - T.start > TREE_LEAF && level < TREE_LEVELS) {
+            if (T.end - T.start > TREE_LEAF && level < levels) {
                 int b[9];
-                child_bounds(T, level, keys, b);
+                child_bounds(T, level, levels, keys, b);
                 for (int d = 0; d < 8; d++) c += b[d + 1] > b[d] ? 1 : 0;
             }
         }
@@ -106,15 +107,15 @@ __global__ void k_tree_next(int level, int cap, int *lv, const int *cnt, const i
     }
 }
 
-__device__ void emit_children(int i, int l0, int level, int next_base, TreeNode *nodes,
-                              const unsigned long long *keys, const int *cnt, const int *off,
-                              unsigned char *gflag)
+__device__ void emit_children(int i, int l0, int level, int levels, int next_base,
+                              TreeNode *nodes, const unsigned long long *keys, const int *cnt,
+                              const int *off, unsigned char *gflag)
 {
     const int c = cnt[i - l0];
     if (c == 0) return;
     TreeNode T = nodes[i];
     int b[9];
-    child_bounds(T, level, keys, b);
+    child_bounds(T, level, levels, keys, b);
     int k = next_base + off[i - l0];
     T.child = k;
     T.nchild = c;
@@ -153,7 +154,7 @@ __device__ void emit_children(int i, int l0, int level, int next_base, TreeNode 
     if (run >= 0) gflag[run] = (unsigned char)run_len;
 }
 
-__global__ void k_tree_emit(int level, const int *lv, TreeNode *nodes,
+__global__ void k_tree_emit(int level, int levels, const int *lv, TreeNode *nodes,
                             const unsigned long long *keys, const int *cnt, const int *off,
                             unsigned char *gflag)
 {
@@ -161,7 +162,7 @@ __global__ void k_tree_emit(int level, const int *lv, TreeNode *nodes,
     if (lv[level + 2] == l1) return;  // no children (or no room: overflow is flagged)
     for (int i = l0 + blockIdx.x * blockDim.x + threadIdx.x; i < l1;
          i += gridDim.x * blockDim.x)
-        emit_children(i, l0, level, l1, nodes, keys, cnt, off, gflag);
+        emit_children(i, l0, level, levels, l1, nodes, keys, cnt, off, gflag);
 }
 
 // Walking groups: runs of consecutive sibling nodes that together hold at
@@ -169,9 +170,10 @@ __global__ void k_tree_emit(int level, const int *lv, TreeNode *nodes,
 // neighbours), and TREE_GROUP-particle chunks of the (coincident-particle)
 // leaves that hold more; each particle lies in exactly one.  Atomic order:
 // results do not depend on which warp walks which group.
-__global__ void k_tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag,
+__global__ void k_tree_groups(DevCount nnc, const TreeNode *nodes, const unsigned char *gflag,
                               int2 *glist, int *count)
 {
+    const int nn = nnc.get();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
         const TreeNode T = nodes[i];
         if (gflag[i]) {
@@ -183,18 +185,39 @@ __global__ void k_tree_groups(int nn, const TreeNode *nodes, const unsigned char
     }
 }
 
-__global__ void k_tree_root(TreeNode *nodes, int n, unsigned char *gflag, int *lv)
+// Level 0: one root per set over the set's sorted slots (its pads excluded);
+// a set of at most TREE_GROUP particles is one walking group.
+__global__ void k_tree_roots(TreeNode *nodes, const SetDesc *sets, int nsets,
+                             unsigned char *gflag, int *lv)
 {
-    lv[0] = 0;
-    lv[1] = 1;
-    lv[TREE_LV_OVERFLOW] = 0;
-    gflag[0] = n <= TREE_GROUP;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) {
+        lv[0] = 0;
+        lv[1] = nsets;
+        lv[TREE_LV_OVERFLOW] = 0;
+    }
+    if (s >= nsets) return;
+    const SetDesc S = sets[s];
+    gflag[s] = S.n > 0 && S.n <= TREE_GROUP;
     TreeNode R;
-    R.start = 0;
-    R.end = n;
+    R.start = S.poff;
+    R.end = S.poff + S.n;
     R.child = 0;
     R.nchild = 0;
-    nodes[0] = R;
+    nodes[s] = R;
+}
+
+// Root (set) of a sorted slot: the last root starting at or before it.
+// Roots are in set order; an empty set's root never holds a group.
+__device__ __forceinline__ int root_of(const TreeNode *nodes, int nroots, int slot)
+{
+    int lo = 0, hi = nroots - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (nodes[mid].start <= slot) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 // ------------------------------------------------------------ properties
@@ -221,8 +244,9 @@ __device__ __forceinline__ double warp_max(double v)
     return v;
 }
 
-__global__ void k_tree_leaf_acc(int nn, const TreeNode *nodes, SortedF64 D, NodeAcc *acc)
+__global__ void k_tree_leaf_acc(DevCount nnc, const TreeNode *nodes, SortedF64 D, NodeAcc *acc)
 {
+    const int nn = nnc.get();
     const int lane = threadIdx.x & 31;
     const int nw = gridDim.x * (blockDim.x >> 5);
     for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nn; i += nw) {
@@ -279,86 +303,88 @@ __global__ void k_tree_leaf_acc(int nn, const TreeNode *nodes, SortedF64 D, Node
     }
 }
 
-__global__ void k_tree_inner_acc(int l0, int l1, const TreeNode *nodes, NodeAcc *acc)
+__global__ void k_tree_inner_acc(int level, const int *lv, const TreeNode *nodes, NodeAcc *acc)
 {
-    const int i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= l1) return;
-    const TreeNode T = nodes[i];
-    if (T.nchild == 0) return;
-    NodeAcc A;
-    A.m = 0.0;
-    double mc[3] = {0.0, 0.0, 0.0};
-    A.h2max = 0.0;
-    for (int d = 0; d < 3; d++) {
-        A.lo[d] = INFINITY;
-        A.hi[d] = -INFINITY;
-    }
-    for (int k = 0; k < T.nchild; k++) {
-        const NodeAcc &C = acc[T.child + k];
-        A.m += C.m;
+    const int l0 = lv[level], l1 = lv[level + 1];
+    for (int i = l0 + blockIdx.x * blockDim.x + threadIdx.x; i < l1; i += gridDim.x * blockDim.x) {
+        const TreeNode T = nodes[i];
+        if (T.nchild == 0) continue;
+        NodeAcc A;
+        A.m = 0.0;
+        double mc[3] = {0.0, 0.0, 0.0};
+        A.h2max = 0.0;
         for (int d = 0; d < 3; d++) {
-            mc[d] += C.m * C.c[d];
-            A.lo[d] = fmin(A.lo[d], C.lo[d]);
-            A.hi[d] = fmax(A.hi[d], C.hi[d]);
+            A.lo[d] = INFINITY;
+            A.hi[d] = -INFINITY;
         }
-        A.h2max = fmax(A.h2max, C.h2max);
+        for (int k = 0; k < T.nchild; k++) {
+            const NodeAcc &C = acc[T.child + k];
+            A.m += C.m;
+            for (int d = 0; d < 3; d++) {
+                mc[d] += C.m * C.c[d];
+                A.lo[d] = fmin(A.lo[d], C.lo[d]);
+                A.hi[d] = fmax(A.hi[d], C.hi[d]);
+            }
+            A.h2max = fmax(A.h2max, C.h2max);
+        }
+        for (int d = 0; d < 3; d++) A.c[d] = A.m > 0.0 ? mc[d] / A.m : 0.5 * (A.lo[d] + A.hi[d]);
+        for (int q = 0; q < 6; q++) A.s[q] = 0.0;
+        for (int k = 0; k < T.nchild; k++) {
+            const NodeAcc &C = acc[T.child + k];
+            const double dx = C.c[0] - A.c[0], dy = C.c[1] - A.c[1], dz = C.c[2] - A.c[2];
+            A.s[0] += C.s[0] + C.m * dx * dx;
+            A.s[1] += C.s[1] + C.m * dy * dy;
+            A.s[2] += C.s[2] + C.m * dz * dz;
+            A.s[3] += C.s[3] + C.m * dx * dy;
+            A.s[4] += C.s[4] + C.m * dx * dz;
+            A.s[5] += C.s[5] + C.m * dy * dz;
+        }
+        acc[i] = A;
     }
-    for (int d = 0; d < 3; d++) A.c[d] = A.m > 0.0 ? mc[d] / A.m : 0.5 * (A.lo[d] + A.hi[d]);
-    for (int q = 0; q < 6; q++) A.s[q] = 0.0;
-    for (int k = 0; k < T.nchild; k++) {
-        const NodeAcc &C = acc[T.child + k];
-        const double dx = C.c[0] - A.c[0], dy = C.c[1] - A.c[1], dz = C.c[2] - A.c[2];
-        A.s[0] += C.s[0] + C.m * dx * dx;
-        A.s[1] += C.s[1] + C.m * dy * dy;
-        A.s[2] += C.s[2] + C.m * dz * dz;
-        A.s[3] += C.s[3] + C.m * dx * dy;
-        A.s[4] += C.s[4] + C.m * dx * dz;
-        A.s[5] += C.s[5] + C.m * dy * dz;
-    }
-    acc[i] = A;
 }
 
-__global__ void k_tree_finalize(int nn, const NodeAcc *acc, double theta, NodeGeom *geom,
+__global__ void k_tree_finalize(DevCount nnc, const NodeAcc *acc, double theta, NodeGeom *geom,
                                 NodeMP *mp)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nn) return;
-    const NodeAcc A = acc[i];
-    NodeGeom G;
-    G.cx = 0.5 * (A.lo[0] + A.hi[0]);
-    G.cy = 0.5 * (A.lo[1] + A.hi[1]);
-    G.cz = 0.5 * (A.lo[2] + A.hi[2]);
-    // half sizes rounded up by 2^-20 of the coordinates' magnitude, so
-    // that float rounding never lets a node look farther than it is
-    const double c3[3] = {G.cx, G.cy, G.cz};
-    float hs[3];
-    double hmax = 0.0;
-    for (int d = 0; d < 3; d++) {
-        const double h = 0.5 * (A.hi[d] - A.lo[d]);
-        hs[d] = (float)(h + 9.5367e-7 * (fabs(c3[d]) + h));
-        hmax = fmax(hmax, h);
+    const int nn = nnc.get();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        const NodeAcc A = acc[i];
+        NodeGeom G;
+        G.cx = 0.5 * (A.lo[0] + A.hi[0]);
+        G.cy = 0.5 * (A.lo[1] + A.hi[1]);
+        G.cz = 0.5 * (A.lo[2] + A.hi[2]);
+        // half sizes rounded up by 2^-20 of the coordinates' magnitude, so
+        // that float rounding never lets a node look farther than it is
+        const double c3[3] = {G.cx, G.cy, G.cz};
+        float hs[3];
+        double hmax = 0.0;
+        for (int d = 0; d < 3; d++) {
+            const double h = 0.5 * (A.hi[d] - A.lo[d]);
+            hs[d] = (float)(h + 9.5367e-7 * (fabs(c3[d]) + h));
+            hmax = fmax(hmax, h);
+        }
+        G.hx = hs[0];
+        G.hy = hs[1];
+        G.hz = hs[2];
+        const double l = 2.0 * hmax;  // edge length
+        G.op2 = l > 0.0 ? (theta > 0.0 ? (float)((l / theta) * (l / theta)) : INFINITY) : 0.f;
+        G.h2max = (float)A.h2max * 1.000001f;
+        G.pad_ = 0.f;
+        geom[i] = G;
+        NodeMP P;
+        P.mx = A.c[0];
+        P.my = A.c[1];
+        P.mz = A.c[2];
+        P.m = A.m;
+        // traceless quadrupole Q = 3 S - tr(S) I
+        const double tr = A.s[0] + A.s[1] + A.s[2];
+        P.q[0] = (float)(3.0 * A.s[0] - tr);
+        P.q[1] = (float)(3.0 * A.s[1] - tr);
+        P.q[2] = (float)(3.0 * A.s[2] - tr);
+        for (int q = 3; q < 6; q++) P.q[q] = (float)(3.0 * A.s[q]);
+        P.pad_[0] = P.pad_[1] = 0.f;
+        mp[i] = P;
     }
-    G.hx = hs[0];
-    G.hy = hs[1];
-    G.hz = hs[2];
-    const double l = 2.0 * hmax;  // edge length
-    G.op2 = l > 0.0 ? (theta > 0.0 ? (float)((l / theta) * (l / theta)) : INFINITY) : 0.f;
-    G.h2max = (float)A.h2max * 1.000001f;
-    G.pad_ = 0.f;
-    geom[i] = G;
-    NodeMP P;
-    P.mx = A.c[0];
-    P.my = A.c[1];
-    P.mz = A.c[2];
-    P.m = A.m;
-    // traceless quadrupole Q = 3 S - tr(S) I
-    const double tr = A.s[0] + A.s[1] + A.s[2];
-    P.q[0] = (float)(3.0 * A.s[0] - tr);
-    P.q[1] = (float)(3.0 * A.s[1] - tr);
-    P.q[2] = (float)(3.0 * A.s[2] - tr);
-    for (int q = 3; q < 6; q++) P.q[q] = (float)(3.0 * A.s[q]);
-    P.pad_[0] = P.pad_[1] = 0.f;
-    mp[i] = P;
 }
 
 // -------------------------------------------------------------------- walk
@@ -388,12 +414,13 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
     int *ps = s_pslot[w];
     int *q = s_q[w];
     double(*qr)[32] = s_qres[w];
+    const int ngroups = a.ngroups_dev ? *a.ngroups_dev : a.ngroups;
 
     for (;;) {
         int g = 0;
         if (lane == 0) g = atomicAdd(a.head, 1);
         g = __shfl_sync(FULL, g, 0);
-        if (g >= a.ngroups) break;
+        if (g >= ngroups) break;
         const int2 grp = a.groups[g];
         const int s0 = grp.x;
         const int s = s0 + lane;
@@ -422,7 +449,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
         int ncell = 0, nfar = 0, npart = 0, top = 1;
         int taken = 0;  // tested-list entries of this group so far
         bool overflow = false, heavy = false;
-        if (lane == 0) stack[0] = 0;
+        // the walk starts at the root of the group's own set
+        if (lane == 0) stack[0] = a.nroots > 1 ? root_of(a.nodes, a.nroots, s0) : 0;
         __syncwarp();
 
         // Every accepted node's box is disjoint from the group's (its gap is
@@ -674,103 +702,174 @@ __global__ void __launch_bounds__(WALK_WARPS * 32) k_tree_walk(TreeWalkArgs a)
 // particles (lane = row) over source chunk c (the block's warps take
 // interleaved sources); warps combine in order, chunks merge in order.
 constexpr int HEAVY_WARPS = 8;
+// Block b works on (heavy group, source chunk) pairs b, b + grid, ...: chunk c
+// of the group's own set, one row per lane, sources split over the warps.
+// The chunk count follows the number of heavy groups (read on the device).
 __global__ void __launch_bounds__(HEAVY_WARPS * 32)
-k_tree_heavy(const int *heavy, const int2 *groups, SortedF64 D, int n, int nkernel, int nchunks,
-             double *partials)
+k_tree_heavy(const int *nheavy_p, int cap, const int *heavy, const int2 *groups,
+             const TreeNode *nodes, int nroots, SortedF64 D, int max_n, int nkernel,
+             double *partials, int *err)
 {
     __shared__ double sh[HEAVY_WARPS][4][32];
-    const int h = blockIdx.x, c = blockIdx.y;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int2 grp = groups[heavy[h]];
-    const int si = grp.x + lane;
-    const bool act = si < grp.y;
-    const int jb = (int)((long long)n * c / nchunks);
-    const int je = (int)((long long)n * (c + 1) / nchunks);
-    double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
-    if (act) {
-        const double xi = D.x[si], yi = D.y[si], zi = D.z[si], h2i = D.h2[si];
-        for (int j = jb + w; j < je; j += HEAVY_WARPS) {
-            const PairOut o = pair_f64_fast(D, nkernel, si, j, D.x[j] - xi, D.y[j] - yi,
-                                            D.z[j] - zi, D.m[j], h2i, D.h2[j]);
-            sx += o.ax;
-            sy += o.ay;
-            sz += o.az;
-            sp += o.pot;
+    const int nh_all = *nheavy_p;
+    if (nh_all > cap && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, DEVERR_TREE_CAP);
+    const int nheavy = min(nh_all, cap);
+    const int nchunks = tree_heavy_chunks(nheavy, max_n);
+    for (int b = blockIdx.x; b < nheavy * nchunks; b += gridDim.x) {
+        const int h = b / nchunks, c = b % nchunks;
+        const int2 grp = groups[heavy[h]];
+        const TreeNode R = nodes[nroots > 1 ? root_of(nodes, nroots, grp.x) : 0];
+        const int ns = R.end - R.start;
+        const int si = grp.x + lane;
+        const bool act = si < grp.y;
+        const int jb = R.start + (int)((long long)ns * c / nchunks);
+        const int je = R.start + (int)((long long)ns * (c + 1) / nchunks);
+        double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+        if (act) {
+            const double xi = D.x[si], yi = D.y[si], zi = D.z[si], h2i = D.h2[si];
+            for (int j = jb + w; j < je; j += HEAVY_WARPS) {
+                const PairOut o = pair_f64_fast(D, nkernel, si, j, D.x[j] - xi, D.y[j] - yi,
+                                                D.z[j] - zi, D.m[j], h2i, D.h2[j]);
+                sx += o.ax;
+                sy += o.ay;
+                sz += o.az;
+                sp += o.pot;
+            }
         }
-    }
-    sh[w][0][lane] = sx;
-    sh[w][1][lane] = sy;
-    sh[w][2][lane] = sz;
-    sh[w][3][lane] = sp;
-    __syncthreads();
-    if (w == 0) {
-        for (int q = 0; q < 4; q++) {
-            double v = sh[0][q][lane];
-            for (int k = 1; k < HEAVY_WARPS; k++) v += sh[k][q][lane];
-            partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane] = v;
+        __syncthreads();  // the previous pair's reduction has read sh
+        sh[w][0][lane] = sx;
+        sh[w][1][lane] = sy;
+        sh[w][2][lane] = sz;
+        sh[w][3][lane] = sp;
+        __syncthreads();
+        if (w == 0) {
+            for (int q = 0; q < 4; q++) {
+                double v = sh[0][q][lane];
+                for (int k = 1; k < HEAVY_WARPS; k++) v += sh[k][q][lane];
+                partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane] = v;
+            }
         }
     }
 }
 
-// warp q of block h: quantity q of heavy group h, chunks in order
-__global__ void k_tree_heavy_merge(int nheavy, const int *heavy, const int2 *groups, int nchunks,
-                                   const double *partials, int n, double *out)
+// warp q of a block: quantity q of heavy group h, chunks in order
+__global__ void k_tree_heavy_merge(const int *nheavy_p, int cap, const int *heavy,
+                                   const int2 *groups, int max_n, const double *partials,
+                                   int nslots, double *out)
 {
-    const int h = blockIdx.x, lane = threadIdx.x & 31, q = threadIdx.x >> 5;
-    if (h >= nheavy) return;
-    const int2 grp = groups[heavy[h]];
-    const int si = grp.x + lane;
-    if (si >= grp.y) return;
-    double v = 0.0;
-    for (int c = 0; c < nchunks; c++) v += partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane];
-    out[(size_t)q * n + si] = v;
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    const int nheavy = min(*nheavy_p, cap);
+    const int nchunks = tree_heavy_chunks(nheavy, max_n);
+    for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
+        const int2 grp = groups[heavy[h]];
+        const int si = grp.x + lane;
+        if (si >= grp.y) continue;
+        double v = 0.0;
+        for (int c = 0; c < nchunks; c++)
+            v += partials[(((size_t)h * nchunks + c) * 4 + q) * 32 + lane];
+        out[(size_t)q * nslots + si] = v;
+    }
 }
 
-cudaError_t tree_heavy(int nheavy, const int *heavy, const int2 *groups, const SortedF64 &D, int n,
-                       int nkernel, double *partials, double *out, cudaStream_t st)
+size_t tree_heavy_partials(int cap, int max_n)
 {
-    if (nheavy <= 0) return cudaSuccess;
-    const int nchunks = tree_heavy_chunks(nheavy, n);
-    k_tree_heavy<<<dim3(nheavy, nchunks), HEAVY_WARPS * 32, 0, st>>>(heavy, groups, D, n, nkernel,
-                                                                    nchunks, partials);
+    // nheavy * tree_heavy_chunks(nheavy, .) <= 4096 + nheavy for every nheavy <= cap
+    (void)max_n;
+    return ((size_t)4096 + (size_t)cap) * 4 * 32;
+}
+
+cudaError_t tree_heavy(int nheavy_host, const int *nheavy, int cap, const int *heavy,
+                       const int2 *groups, const TreeNode *nodes, int nroots, const SortedF64 &D,
+                       int nslots, int max_n, int nkernel, double *partials, double *out, int *err,
+                       cudaStream_t st)
+{
+    // eager calls know the count: one block per (group, chunk); captured
+    // calls size the grid for the most chunks any count can give
+    const int blocks = nheavy_host > 0
+                           ? std::min(nheavy_host, cap) * tree_heavy_chunks(std::min(nheavy_host, cap), max_n)
+                           : 4096;
+    k_tree_heavy<<<blocks, HEAVY_WARPS * 32, 0, st>>>(nheavy, cap, heavy, groups, nodes, nroots, D,
+                                                     max_n, nkernel, partials, err);
     ++g_launches;
-    k_tree_heavy_merge<<<nheavy, 128, 0, st>>>(nheavy, heavy, groups, nchunks, partials, n, out);
+    const int mblocks = nheavy_host > 0 ? std::min(nheavy_host, cap) : 256;
+    k_tree_heavy_merge<<<mblocks, 128, 0, st>>>(nheavy, cap, heavy, groups, max_n, partials, nslots,
+                                               out);
     ++g_launches;
     return cudaGetLastError();
 }
 
-// Sorted-order results to the caller's rows [i_lo, i_lo + ni).
-__global__ void k_tree_scatter(int n, int i_lo, int ni, const double *res, const int *orig,
+// Sorted-order results to the caller's rows [i_lo, i_lo + ni) (pad slots,
+// orig < 0, are skipped).
+__global__ void k_tree_scatter(int nslots, int i_lo, int ni, const double *res, const int *orig,
                                OutputsDev out)
 {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
         const int p = orig[s];
         if (p < i_lo || p >= i_lo + ni) continue;
         out.ax[p] = res[s];
-        out.ay[p] = res[n + s];
-        out.az[p] = res[2 * n + s];
-        out.pot[p] = res[3 * n + s];
+        out.ay[p] = res[nslots + s];
+        out.az[p] = res[2 * nslots + s];
+        out.pot[p] = res[3 * nslots + s];
     }
 }
 
-// W = 1/2 sum m phi over the particles, one block, fixed order.
-__global__ void k_tree_wsum(int n, const double *res, const double *m, double *W)
+// W = 1/2 sum m phi over each set's particles: one block per set, fixed order.
+__global__ void k_tree_wsum(const SetDesc *sets, int nslots, const double *res, const double *m,
+                            double *W)
 {
     __shared__ double part[1024];
+    const SetDesc S = sets[blockIdx.x];
     double w = 0.0;
-    for (int s = threadIdx.x; s < n; s += blockDim.x) w += m[s] * res[3 * n + s];
+    for (int k = threadIdx.x; k < S.n; k += blockDim.x)
+        w += m[S.poff + k] * res[3 * (size_t)nslots + S.poff + k];
     part[threadIdx.x] = w;
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
         if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) *W = 0.5 * part[0];
+    if (threadIdx.x == 0) W[blockIdx.x] = 0.5 * part[0];
 }
 
-cudaError_t tree_wsum(int n, const double *res, const double *m, double *W, cudaStream_t st)
+cudaError_t tree_wsum(const SetDesc *sets, int nsets, int nslots, const double *res,
+                      const double *m, double *W, cudaStream_t st)
 {
-    k_tree_wsum<<<1, 1024, 0, st>>>(n, res, m, W);
+    if (nsets <= 0) return cudaSuccess;
+    k_tree_wsum<<<nsets, 1024, 0, st>>>(sets, nslots, res, m, W);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+// Keys by sorted slot: set s's particles sit at slots [poff, poff + n) and
+// at [off, off + n) of the sorted key array.
+__global__ void k_tree_slot_keys(const SetDesc *sets, const unsigned long long *keys_sorted,
+                                 unsigned long long *keys_slot)
+{
+    const SetDesc S = sets[blockIdx.y];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S.n; k += gridDim.x * blockDim.x)
+        keys_slot[S.poff + k] = keys_sorted[S.off + k];
+}
+
+cudaError_t tree_slot_keys(const SetDesc *sets, int nsets, int max_n,
+                           const unsigned long long *keys_sorted, unsigned long long *keys_slot,
+                           cudaStream_t st)
+{
+    if (nsets <= 0 || max_n <= 0) return cudaSuccess;
+    const dim3 grid(std::min((max_n + 255) / 256, 1024), nsets);
+    k_tree_slot_keys<<<grid, 256, 0, st>>>(sets, keys_sorted, keys_slot);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+__global__ void k_tree_check_build(const int *lv, int *err)
+{
+    if (lv[TREE_LV_OVERFLOW]) atomicOr(err, DEVERR_TREE_CAP);
+}
+
+cudaError_t tree_check_build(const int *lv, int *err, cudaStream_t st)
+{
+    k_tree_check_build<<<1, 1, 0, st>>>(lv, err);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -787,14 +886,16 @@ cudaError_t tree_build_levels(const TreeBuildArgs &t, int level_begin, int level
                               cudaStream_t st)
 {
     if (level_begin == 0) {
-        k_tree_root<<<1, 1, 0, st>>>(t.nodes, t.n, t.gflag, t.lv);
+        k_tree_roots<<<(t.nroots + 127) / 128, 128, 0, st>>>(t.nodes, t.sets, t.nroots, t.gflag, t.lv);
         ++g_launches;
     }
     for (int level = level_begin; level < level_end; level++) {
-        // level has at most min(8^level, n) nodes
-        const int bound = (int)std::min<long long>(1ll << (3 * level), (long long)std::max(t.n, 1));
+        // level has at most min(roots * 8^level, n) nodes
+        const long long fan = level < 20 ? (1ll << (3 * level)) : (1ll << 60);
+        const long long b = (long long)t.nroots * std::min(fan, (long long)t.n);
+        const int bound = (int)std::max(1ll, std::min(b, (long long)std::max(t.n, 1)));
         const int blocks = std::min((bound + 255) / 256, 4096);
-        k_tree_count<<<blocks, 256, 0, st>>>(level, bound, t.lv, t.nodes, t.keys, t.cnt);
+        k_tree_count<<<blocks, 256, 0, st>>>(level, t.levels, bound, t.lv, t.nodes, t.keys, t.cnt);
         ++g_launches;
         size_t tb = t.scan_temp_bytes;
         const cudaError_t e = cub::DeviceScan::ExclusiveSum(t.scan_temp, tb, t.cnt, t.off, bound, st);
@@ -802,18 +903,24 @@ cudaError_t tree_build_levels(const TreeBuildArgs &t, int level_begin, int level
         ++g_launches;
         k_tree_next<<<1, 1, 0, st>>>(level, t.cap, t.lv, t.cnt, t.off);
         ++g_launches;
-        k_tree_emit<<<blocks, 256, 0, st>>>(level, t.lv, t.nodes, t.keys, t.cnt, t.off, t.gflag);
+        k_tree_emit<<<blocks, 256, 0, st>>>(level, t.levels, t.lv, t.nodes, t.keys, t.cnt, t.off,
+                                            t.gflag);
         ++g_launches;
     }
     return cudaGetLastError();
 }
 
-cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gflag, int2 *glist,
-                        int *count, cudaStream_t st)
+static int grid_for(DevCount c, int per_block, int cap_blocks)
+{
+    return std::max(1, std::min((std::max(c.host, 1) + per_block - 1) / per_block, cap_blocks));
+}
+
+cudaError_t tree_groups(DevCount nn, const TreeNode *nodes, const unsigned char *gflag,
+                        int2 *glist, int *count, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    k_tree_groups<<<std::min((nn + 255) / 256, 4096), 256, 0, st>>>(nn, nodes, gflag, glist, count);
+    k_tree_groups<<<grid_for(nn, 256, 4096), 256, 0, st>>>(nn, nodes, gflag, glist, count);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -821,15 +928,22 @@ cudaError_t tree_groups(int nn, const TreeNode *nodes, const unsigned char *gfla
 // Walking order: the largest H first.  Every particle within H of a group
 // is tested pair by pair, so those groups walk longest; started first, they
 // do not leave one warp running after the rest (results do not depend on the
-// order: each group's sums are its own).
-__global__ void k_tree_group_keys(int ng, const int2 *glist, const double *h2, unsigned *keys)
+// order: each group's sums are its own).  Entries past the group count (a
+// device count bounded by ng.host) get key 0 and sort last.
+__global__ void k_tree_group_keys(DevCount ngc, int bound, const int2 *glist, const double *h2,
+                                  unsigned *keys)
 {
+    const int ng = ngc.get();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ng) return;
-    const int2 r = glist[g];
+    if (g >= bound) return;
     double m = 0.0;
-    for (int s = r.x; s < r.y; s++) m = fmax(m, h2[s]);
-    keys[g] = __float_as_uint((float)m);  // non-negative floats order as their bits
+    if (g < ng) {
+        const int2 r = glist[g];
+        for (int s = r.x; s < r.y; s++) m = fmax(m, h2[s]);
+    }
+    // non-negative floats order as their bits; a group always keys above
+    // the unused entries, even if its H^2 rounds to a float 0
+    keys[g] = g < ng ? max(__float_as_uint((float)m), 1u) : 0u;
 }
 
 size_t tree_order_temp_bytes(int ng)
@@ -837,39 +951,44 @@ size_t tree_order_temp_bytes(int ng)
     size_t bytes = 0;
     cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const unsigned *)nullptr,
                                               (unsigned *)nullptr, (const int2 *)nullptr,
-                                              (int2 *)nullptr, ng);
+                                              (int2 *)nullptr, std::max(ng, 1));
     return bytes;
 }
 
-cudaError_t tree_order_groups(int ng, const int2 *glist, int2 *ordered, const double *h2,
+cudaError_t tree_order_groups(DevCount ng, const int2 *glist, int2 *ordered, const double *h2,
                               unsigned *keys_in, unsigned *keys_out, void *temp, size_t temp_bytes,
                               cudaStream_t st)
 {
-    if (ng <= 0) return cudaSuccess;
-    k_tree_group_keys<<<(ng + 255) / 256, 256, 0, st>>>(ng, glist, h2, keys_in);
+    if (ng.host <= 0) return cudaSuccess;
+    k_tree_group_keys<<<(ng.host + 255) / 256, 256, 0, st>>>(ng, ng.host, glist, h2, keys_in);
     ++g_launches;
     size_t tb = temp_bytes;
     const cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(temp, tb, keys_in, keys_out,
-                                                                    glist, ordered, ng, 0, 32, st);
+                                                                    glist, ordered, ng.host, 0, 32,
+                                                                    st);
     ++g_launches;
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 size_t tree_acc_bytes(int nn) { return (size_t)nn * sizeof(NodeAcc); }
 
-cudaError_t tree_props(int nn, const TreeNode *nodes, const SortedF64 &D, double theta,
-                       const int *level_start, int depth, void *acc_buf, NodeGeom *geom,
-                       NodeMP *mp, cudaStream_t st)
+cudaError_t tree_props(DevCount nn, const TreeNode *nodes, const SortedF64 &D, double theta,
+                       const int *lv, const int *level_start, int depth, int level_bound,
+                       void *acc_buf, NodeGeom *geom, NodeMP *mp, cudaStream_t st)
 {
     NodeAcc *acc = (NodeAcc *)acc_buf;
-    k_tree_leaf_acc<<<std::min((nn + 7) / 8, 148 * 16), 256, 0, st>>>(nn, nodes, D, acc);
+    k_tree_leaf_acc<<<grid_for(nn, 8, 148 * 16), 256, 0, st>>>(nn, nodes, D, acc);
     ++g_launches;
     for (int l = depth - 1; l >= 0; l--) {
-        const int l0 = level_start[l], l1 = level_start[l + 1];
-        k_tree_inner_acc<<<(l1 - l0 + 127) / 128, 128, 0, st>>>(l0, l1, nodes, acc);
+        // a level's node count: exact when the host read the level table,
+        // else bounded (grid-stride)
+        const int cnt = level_start ? level_start[l + 1] - level_start[l] : level_bound;
+        if (level_start && cnt <= 0) continue;
+        k_tree_inner_acc<<<std::max(1, std::min((cnt + 127) / 128, 148 * 8)), 128, 0, st>>>(
+            l, lv, nodes, acc);
         ++g_launches;
     }
-    k_tree_finalize<<<(nn + 255) / 256, 256, 0, st>>>(nn, acc, theta, geom, mp);
+    k_tree_finalize<<<grid_for(nn, 256, 148 * 16), 256, 0, st>>>(nn, acc, theta, geom, mp);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -883,10 +1002,11 @@ cudaError_t tree_walk(const TreeWalkArgs &a, int sm_count, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t tree_scatter(int n, int i_lo, int ni, const double *res, const int *orig,
+cudaError_t tree_scatter(int nslots, int i_lo, int ni, const double *res, const int *orig,
                          const OutputsDev &out, cudaStream_t st)
 {
-    k_tree_scatter<<<std::min((n + 255) / 256, 4096), 256, 0, st>>>(n, i_lo, ni, res, orig, out);
+    k_tree_scatter<<<std::max(1, std::min((nslots + 255) / 256, 4096)), 256, 0, st>>>(
+        nslots, i_lo, ni, res, orig, out);
     ++g_launches;
     return cudaGetLastError();
 }

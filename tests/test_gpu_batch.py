@@ -261,3 +261,30 @@ def test_reference_gpu_library_is_less_accurate(gpu_ctx):
     # compare the typical error
     assert r_our["pot_rms"] <= r_ref["pot_rms"]
     assert r_our["pot_max"] <= 2 * r_ref["pot_max"]
+
+
+def test_graph_destroyed_during_another_capture(gpu_ctx):
+    """Releasing a graph while the same thread captures another one (what a
+    garbage-collected handle does) waits until the capture ends instead of
+    invalidating it."""
+    from starsmasher_b200 import _lib
+    t = _t()
+    b = inputs.collision_snapshots(2, 2000, 3000, seed=53)
+    X = [dev(a) for a in (b.x, b.y, b.z, b.m, b.range2)]
+    outs = [t.zeros(b.n, dtype=t.float64, device="cuda") for _ in range(4)]
+    gpu_ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")
+    gpu_ctx.sync()
+    want = [o.cpu().numpy() for o in outs]
+    with gpu_ctx.capture() as first:
+        gpu_ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")
+    with gpu_ctx.capture() as second:
+        _lib.load().sphgrav_graph_destroy(first.graph._h)
+        first.graph._h = None
+        gpu_ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")
+    for o in outs:
+        o.zero_()
+    second.graph.launch(1)
+    gpu_ctx.sync()
+    for o, w in zip(outs, want):
+        assert np.array_equal(o.cpu().numpy(), w)
+

@@ -11,7 +11,9 @@ equality:
 and check what must hold exactly: bit-for-bit reproducible results, row
 slices equal to the full call's rows, groups handed to the direct FP64 sum
 (a point-mass core whose softening sphere holds most of the star) exact to
-1e-10, and the calls that tree mode refuses.
+1e-10, batches (one root per set: sets never see each other) and CUDA-graph
+capture (every count kept on the device) equal to the eager single-set
+calls, and the calls that tree mode refuses.
 """
 import json
 import os
@@ -200,23 +202,118 @@ def test_refusals(gpu_ctx, star16k):
         with pytest.raises(_lib.SphgravError) as e:
             gpu_ctx.set_theta(bad)
         assert e.value.status == _lib.ERR_INVALID_ARGUMENT
-    b = inputs.batch_models(3, 500, 1500, seed=71)
-    with pytest.raises(_lib.SphgravError) as e:
-        gpu_ctx.batch_forces(b.offsets, b.x, b.y, b.z, b.m, b.range2, 0, "tree")
-    assert e.value.status == _lib.ERR_INVALID_ARGUMENT
+    # a capture of a tree call of sizes no eager call has prepared
+    from starsmasher_b200 import Context
     t = _torch()
     X = [dev(a) for a in (s.x, s.y, s.z, s.m, s.range2)]
     outs = [t.zeros(s.n, dtype=t.float64, device="cuda") for _ in range(4)]
-    gpu_ctx.forces_device(s.n, *X, *outs, precision="tree")
-    gpu_ctx.sync()
-    with pytest.raises(_lib.SphgravError) as e:
-        with gpu_ctx.capture():
-            gpu_ctx.forces_device(s.n, *X, *outs, precision="tree")
-    assert e.value.status == _lib.ERR_PROTOCOL
-    gpu_ctx.sync()
-    # the context stays usable
-    got = _tree(gpu_ctx, s, 0.5)
-    assert np.all(np.isfinite(got[0]))
+    with Context(0) as fresh:
+        with pytest.raises(_lib.SphgravError) as e:
+            with fresh.capture():
+                fresh.forces_device(s.n, *X, *outs, precision="tree")
+        assert e.value.status == _lib.ERR_PROTOCOL
+        fresh.sync()
+        # the context stays usable
+        got = _tree(fresh, s, 0.5)
+        assert np.all(np.isfinite(got[0]))
+
+
+def _two_copies(s):
+    """A batch of two identical copies of one model (same positions)."""
+    cat = lambda a: np.concatenate([a, a])
+    return cat(s.x), cat(s.y), cat(s.z), cat(s.m), cat(s.range2), np.array([0, s.n, 2 * s.n])
+
+
+def test_batch_sets_never_see_each_other(gpu_ctx, star16k):
+    """Two copies of a model at the same positions in one batch: each set's
+    tree has its own root, so each copy gets exactly the single-set answer
+    (an interaction across sets would double the forces)."""
+    s = star16k
+    single = _tree(gpu_ctx, s, 0.3)
+    x, y, z, m, r2, offs = _two_copies(s)
+    gpu_ctx.set_theta(0.3)
+    res = gpu_ctx.batch_forces(offs, x, y, z, m, r2, 0, "tree")
+    for q in range(4):
+        assert np.array_equal(res[q][: s.n], single[q])
+        assert np.array_equal(res[q][s.n:], single[q])
+
+
+def test_batch_of_uneven_models(gpu_ctx):
+    """A batch of uneven models, an empty set and a set smaller than one
+    walking group, against the FP64 direct sum of each model, and W per set."""
+    b = inputs.batch_models(5, 500, 6000, seed=71)
+    parts = [(b.x[b.offsets[k]:b.offsets[k + 1]], b.y[b.offsets[k]:b.offsets[k + 1]],
+              b.z[b.offsets[k]:b.offsets[k + 1]], b.m[b.offsets[k]:b.offsets[k + 1]],
+              b.range2[b.offsets[k]:b.offsets[k + 1]]) for k in range(b.nsets)]
+    parts.insert(2, tuple(np.zeros(0) for _ in range(5)))
+    # 20 particles of the first model (its smoothing lengths): one walking group
+    parts.append(tuple(np.array(a[:20]) for a in parts[0]))
+    offs = np.cumsum([0] + [len(p[0]) for p in parts])
+    cols = [np.concatenate([p[q] for p in parts]) for q in range(5)]
+    gpu_ctx.set_theta(0.3)
+    out = gpu_ctx.batch_forces(offs, *cols, 0, "tree")
+    res, W = out[:4], out[4]
+    rms_b, max_b, pot_b = BOUNDS[0.3]
+    for k in range(len(parts)):
+        a, e = offs[k], offs[k + 1]
+        if e == a:
+            assert W[k] == 0.0
+            continue
+        want = gpu_ctx.forces(*(c[a:e] for c in cols), 0, "fp64")
+        r = err_report(res[0][a:e], res[1][a:e], res[2][a:e], res[3][a:e], *want)
+        assert r["acc_rms"] <= rms_b and r["acc_max"] <= max_b and r["pot_rms"] <= pot_b, (k, r)
+        w_want = 0.5 * np.sum(cols[3][a:e] * res[3][a:e])
+        assert abs(W[k] - w_want) <= 1e-12 * abs(w_want), (k, W[k], w_want)
+
+
+def test_captured_tree_sweep_matches_eager(gpu_ctx):
+    """kick + tree gravity captured once (the build issues every key level,
+    the group and hand-off counts stay on the device) and replayed == the
+    same calls issued eagerly, on one set and on a batch."""
+    t = _torch()
+    for b in (inputs.collision_snapshots(1, 6000, 6000, seed=81),
+              inputs.collision_snapshots(3, 2000, 5000, seed=82)):
+        n = b.n
+        sigma, seed = 1e-3, 99
+
+        def fresh():
+            return [dev(a) for a in (b.x, b.y, b.z, b.m, b.range2)]
+
+        def call(X, outs, W):
+            if b.nsets == 1:
+                gpu_ctx.forces_device(n, *X, *outs, W=W, precision="tree")
+            else:
+                gpu_ctx.batch_forces_device(b.offsets, *X, *outs, W=W, precision="tree")
+
+        gpu_ctx.set_theta(0.5)
+        try:
+            X = fresh()
+            outs_e = [t.zeros(n, dtype=t.float64, device="cuda") for _ in range(4)]
+            W_e = t.zeros(b.nsets, dtype=t.float64, device="cuda")
+            gpu_ctx.kick_reset(0)
+            for _ in range(3):
+                gpu_ctx.kick_device(n, X[0], X[1], X[2], sigma, seed)
+                call(X, outs_e, W_e)
+            gpu_ctx.sync()
+            res_e = [a.cpu().numpy() for a in outs_e] + [W_e.cpu().numpy()]
+
+            X = fresh()
+            outs = [t.zeros(n, dtype=t.float64, device="cuda") for _ in range(4)]
+            W = t.zeros(b.nsets, dtype=t.float64, device="cuda")
+            gpu_ctx.kick_reset(0)
+            call(X, outs, W)  # sizes the buffers
+            gpu_ctx.sync()
+            with gpu_ctx.capture() as cap:
+                gpu_ctx.kick_device(n, X[0], X[1], X[2], sigma, seed)
+                call(X, outs, W)
+            cap.graph.launch(3)
+            gpu_ctx.sync()
+            for a, r in zip([a.cpu().numpy() for a in outs] + [W.cpu().numpy()], res_e):
+                assert np.array_equal(a, r)
+            groups, heavy = gpu_ctx.tree_stats()
+            assert groups == -1 and heavy == -1  # counts of a captured call stay on the device
+        finally:
+            gpu_ctx.set_theta(0.3)
 
 
 def test_legacy_abi_takes_theta_from_gpu_init_dev(gpu_ctx, star16k):
