@@ -358,6 +358,40 @@ def config4_section(torch, ctx, timer, device, args):
             "l2": "flushed before every timed call"}
 
 
+def single_set_section(torch, ctx, timer, device, args, name):
+    """A single-set benchmark workload other than the headline one (config1,
+    config2): split-FP32 whole-call rate, its pair kernel's share of the
+    FP32 peak probe, the FP64 kernel's rate and the accuracy against it."""
+    ws = load_workload(name)
+    X, outs = upload(torch, ws, device)
+
+    def call(prec="f32split"):
+        ctx.forces_device(ws.n, *X, *outs, nkernel=args.nkernel, precision=prec)
+
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    ctx.profile_enable(True)
+    ctx.profile_read()
+    ms = timer.run(call, 5)
+    kern_ms, kern_n = ctx.profile_read()
+    ctx.profile_enable(False)
+    res32 = [o.cpu().numpy() for o in outs]
+    refined = ctx.last_refine_rows()
+    call("fp64")
+    ms64 = timer.run(lambda: call("fp64"), 2)
+    res64 = [o.cpu().numpy() for o in outs]
+    pairs = ws.pairs
+    kms = kern_ms / max(1, kern_n)
+    return {"workload": ws.name, "n": ws.n, "pairs_per_step": pairs, "ms_per_step": ms,
+            "value": pairs / (ms * 1e-3) / 1e9, "kernel_ms_per_launch": kms,
+            "kernel_tflops": pairs * FLOPS_PER_PAIR / (kms * 1e-3) / 1e12,
+            "fp64_ms_per_step": ms64, "fp64_value": pairs / (ms64 * 1e-3) / 1e9,
+            "speedup_f32split_vs_fp64": ms64 / ms, "refined_rows": refined,
+            "accuracy_vs_fp64": accuracy(res32, res64),
+            "l2": "flushed before every timed step"}
+
+
 def config5_section(torch, ctx, timer, stream, device, args):
     """The graph-captured sweep (config5): a CUDA graph of (seeded position
     kick, sigma = 1e-3 R, + batched gravity) replayed on device-resident
@@ -700,6 +734,8 @@ def main():
     if world == 1 and args.workload == "config3" and not args.no_extras:
         extras["config4_batched"] = config4_section(torch, ctx, timer, device, args)
         extras["config5_graph_sweep"] = config5_section(torch, ctx, timer, stream, device, args)
+        for name in ("config1", "config2"):
+            extras[f"{name}_single_set"] = single_set_section(torch, ctx, timer, device, args, name)
 
     phases = None
     if args.phases and args.precision == "f32split":
