@@ -202,10 +202,10 @@ struct sphgrav_ctx {
     int scale_n = 0;                   // rows of the kept G (0: none)
     int refine_nsets = 0;              // sets of the last split-FP32 call (rcount entries)
     DBuf<float> gpart;                 // [slot][itile] G^2 partials
-    DBuf<int> rcount, rlist, rnitems, rhead;
+    DBuf<int> rcount, rlist, rnitems, rhead, rnlight;
     DBuf<SetDesc> rsets;
-    DBuf<WorkItem> ritems;
-    DBuf<double> rpart, scale;
+    DBuf<WorkItem> ritems, rlitems;  // tile items; row-chunk items of sets with few rows
+    DBuf<double> rpart, scale, rlpart;  // rlpart: row-chunk partials [item][4]
 
     // Barnes-Hut mode (SPHGRAV_TREE)
     double theta = 0.3;   // opening angle (gpu_init_dev_ passes it; main.f:269)
@@ -288,6 +288,12 @@ static const int kMinChunkJ = 2048;  // shortest j-chunk worth a partial slot
 // FP64 variant that recomputes the refine-listed rows (few rows per set: the
 // smallest row tile)
 static const int kRefineVariant = 0;
+// ... and for sets of at most kRefineSmallN particles the 64-source-tile
+// shape with 64-source chunks (16K: 22 rows refined in 76 us with 256-source
+// chunks; their near pairs, one after another per row, set the time)
+static const int kRefineVariantSmall = 12;
+static const int kRefineSmallN = 65536;
+static int refine_variant(const Plan &P) { return P.max_n <= kRefineSmallN ? kRefineVariantSmall : kRefineVariant; }
 
 static int ceil_log2(long long v)
 {
@@ -380,7 +386,7 @@ static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     P.tj = V.tj;
     long long poff = 0, ioff = 0, toff = 0, moff = 0;
     for (int s = 0; s < P.nsets; s++) {
-        SetDesc d;
+        SetDesc d{};
         memset(&d, 0, sizeof(d));
         d.n = offsets[s + 1] - offsets[s];
         d.off = offsets[s];
@@ -583,14 +589,17 @@ static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_ro
         TRY(ensure(c, c->rsets, std::max(1, P.nsets), "refine sets"));
         TRY(ensure(c, c->rnitems, 1, "refine items"));
         TRY(ensure(c, c->rhead, 1, "refine head"));
-        const VariantInfo &V = variant_info(SPHGRAV_FP64, kRefineVariant);
+        const int rv = refine_variant(P);
+        const VariantInfo &V = variant_info(SPHGRAV_FP64, rv);
         long long tiles = 0;
         for (const SetDesc &d : P.sets) tiles += (d.ni + V.itile() - 1) / V.itile();
-        const long long target =
-            4ll * variant_occupancy(SPHGRAV_FP64, kRefineVariant) * c->sm_count;
+        const long long target = 4ll * variant_occupancy(SPHGRAV_FP64, rv) * c->sm_count;
         const size_t cap = (size_t)std::max(1ll, std::max(tiles, target));
         TRY(ensure(c, c->ritems, cap, "refine items"));
         TRY(ensure(c, c->rpart, cap * 4 * V.itile(), "refine partials"));
+        TRY(ensure(c, c->rlitems, REFINE_LIGHT_CAP, "refine row-chunk items"));
+        TRY(ensure(c, c->rlpart, 4 * (size_t)REFINE_LIGHT_CAP, "refine row-chunk partials"));
+        TRY(ensure(c, c->rnlight, 1, "refine row-chunk items"));
         if (c->keep_scale) TRY(ensure(c, c->scale, std::max(1, P.ntot), "error scale"));
     }
     const size_t sb = sort_temp_bytes(P.ntot, P.end_bit);
@@ -821,13 +830,18 @@ static int run_refine(sphgrav_ctx *c, int nkernel, const SortedF64 &D, const Out
 {
     const Plan &P = c->plan;
     cudaStream_t st = c->stream;
-    const int v = kRefineVariant;
+    const int v = refine_variant(P);
     const VariantInfo &V = variant_info(SPHGRAV_FP64, v);
     const int resident = variant_occupancy(SPHGRAV_FP64, v) * c->sm_count;
-    CUDA_TRY(launch_refine_plan(c->sets.p, P.nsets, c->rcount.p, V.itile(), V.tj, 4 * resident,
+    const int min_j = v == kRefineVariantSmall ? 64 : 256;  // sources per refine chunk, at least
+    CUDA_TRY(launch_refine_plan(c->sets.p, P.nsets, c->rcount.p, V.itile(), V.tj, min_j, 4 * resident,
                                 (int)std::min<size_t>(c->ritems.cap, 0x7fffffff), c->rsets.p,
-                                c->ritems.p, c->rnitems.p, c->err.p, st));
+                                c->ritems.p, c->rnitems.p, c->rlitems.p, c->rnlight.p, c->err.p,
+                                st));
     CUDA_TRY(cudaMemsetAsync(c->rhead.p, 0, sizeof(int), st));
+    // sets with few listed rows: one warp per (row, source chunk)
+    CUDA_TRY(launch_refine_light(c->rsets.p, c->rlitems.p, c->rnlight.p, c->rlist.p, D, nkernel,
+                                 c->rlpart.p, c->sm_count, st));
     ComputeArgs a{};
     a.sets = c->rsets.p;
     a.items = c->ritems.p;
@@ -846,7 +860,7 @@ static int run_refine(sphgrav_ctx *c, int nkernel, const SortedF64 &D, const Out
     a.band2 = 1.f;
     CUDA_TRY(launch_compute(SPHGRAV_FP64, v, resident, a, st));
     CUDA_TRY(launch_refine_merge(c->sets.p, c->rsets.p, c->tile_set.p, P.ntiles, P.itile, V.itile(),
-                                 c->rcount.p, c->rlist.p, D, c->rpart.p, out, st));
+                                 c->rcount.p, c->rlist.p, D, c->rpart.p, c->rlpart.p, out, st));
     return SPHGRAV_OK;
 }
 
@@ -1183,6 +1197,7 @@ int sphgrav_destroy(sphgrav_ctx *c)
     c->range2.release();
     c->gpart.release(); c->rcount.release(); c->rlist.release(); c->rnitems.release();
     c->rhead.release(); c->rsets.release(); c->ritems.release(); c->rpart.release();
+    c->rnlight.release(); c->rlitems.release(); c->rlpart.release();
     c->scale.release(); c->phases.release();
     c->tnodes.release(); c->tgeom.release(); c->tmp.release(); c->tcnt.release(); c->tkeys.release();
     c->toff.release(); c->tstack.release(); c->tscan.release(); c->tres.release();

@@ -274,7 +274,10 @@ __global__ void __launch_bounds__(NT, F64Occ<NT, K, MB>::MINB) k_fp64(ComputeArg
 
 // name, threads NT, rows per thread K, j-tile TJ, stages NS, far-loop unroll U,
 // resident blocks per SM the registers are sized for MB (0: by K and NT).
-// Variant 0 (the smallest row tile) also recomputes the split-FP32 refine rows.
+// Variants 0 and 12 (one row per thread, 128- or 64-source tiles) also
+// recompute the split-FP32 refine rows (64-source tiles for sets of at most
+// 65,536 particles: shorter j-chunks spread a few rows' near pairs over more
+// blocks).
 #define SG_F64_VARIANTS(X)                                   \
     X(128, 1, 128, 3, 2, 0, "fp64_nt128_k1_tj128")           \
     X(128, 2, 128, 3, 2, 0, "fp64_nt128_k2_tj128")           \
@@ -287,7 +290,8 @@ __global__ void __launch_bounds__(NT, F64Occ<NT, K, MB>::MINB) k_fp64(ComputeArg
     X(64, 2, 256, 3, 2, 0, "fp64_nt64_k2_tj256")             \
     X(32, 2, 128, 3, 2, 0, "fp64_nt32_k2_tj128")             \
     X(128, 2, 256, 3, 1, 4, "fp64_nt128_k2_tj256_u1_b4")     \
-    X(64, 3, 256, 3, 2, 0, "fp64_nt64_k3_tj256")
+    X(64, 3, 256, 3, 2, 0, "fp64_nt64_k3_tj256")             \
+    X(128, 1, 64, 3, 2, 0, "fp64_nt128_k1_tj64")
 
 #define SG_INFO(NT, K, TJ, NS, U, MB, NAME) {0, NT, K, 1, TJ, 0, NAME, NT * K},
 static const VariantInfo kF64Variants[] = {SG_F64_VARIANTS(SG_INFO)};

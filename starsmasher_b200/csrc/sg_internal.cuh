@@ -27,6 +27,8 @@ struct SetDesc {
     int meta_off;  // first j metadata record of the set
     int slot_off;  // first partial slot of the set (refine plans: of its items)
     int nchunks;   // j-chunks per i-tile (the main plan: the most of any tile)
+    int light_off; // refine plans, sets with few listed rows: first row-chunk item
+    int light_nch; // ... and source chunks per row (0: the set's rows use tiles)
 };
 
 // One unit of the persistent kernels' device-side queue.

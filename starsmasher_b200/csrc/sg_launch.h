@@ -141,9 +141,16 @@ cudaError_t launch_wtile_out(const SetDesc *sets, const int *tile_set, int ntile
 // the refine), the items and their count.  At most max_items items are
 // written; a plan that would need more sets DEVERR_INPUT (never expected:
 // the host sizes max_items for every row flagged).
+// Row-chunk items (sets with at most 32 listed rows: one warp per row and
+// source chunk) a refine plan may hold.
+constexpr int REFINE_LIGHT_CAP = 65536;
 cudaError_t launch_refine_plan(const SetDesc *sets, int nsets, const int *rcount, int itile,
-                               int tj, int target, int max_items, SetDesc *rsets,
-                               WorkItem *items, int *nitems, int *err, cudaStream_t st);
+                               int tj, int min_j, int target, int max_items, SetDesc *rsets,
+                               WorkItem *items, int *nitems, WorkItem *litems, int *nlight,
+                               int *err, cudaStream_t st);
+cudaError_t launch_refine_light(const SetDesc *rsets, const WorkItem *items, const int *nitems,
+                                const int *rlist, const SortedF64 &D, int nkernel, double *lpart,
+                                int sm_count, cudaStream_t st);
 // Scatter the refined rows: chunk sums in chunk order, written over the
 // split-FP32 results in the caller's order.  Launched over the main plan's
 // tiles (grid ntiles_main); tile t covers refine-list entries
@@ -151,7 +158,7 @@ cudaError_t launch_refine_plan(const SetDesc *sets, int nsets, const int *rcount
 cudaError_t launch_refine_merge(const SetDesc *sets, const SetDesc *rsets, const int *tile_set,
                                 int ntiles_main, int itile_main, int itile_ref, const int *rcount,
                                 const int *rlist, const SortedF64 D, const double *rpart,
-                                OutputsDev out, cudaStream_t st);
+                                const double *lpart, OutputsDev out, cudaStream_t st);
 cudaError_t launch_wsum(const SetDesc *sets, int nsets, const double *wtile, double *W,
                         cudaStream_t st);
 cudaError_t launch_range2(int n, const double *hp, const double *u, double *range2, cudaStream_t st);

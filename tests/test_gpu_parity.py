@@ -320,13 +320,19 @@ def test_fp64_band_setting(gpu_ctx, star16k, tri16k, band):
     assert r["acc_max"] <= F32_TOL, r
 
 
-def test_refine_recomputes_listed_rows_in_fp64(gpu_ctx):
+@pytest.mark.parametrize("case", ["tiles", "row_chunks"])
+def test_refine_recomputes_listed_rows_in_fp64(gpu_ctx, case):
     """The FP64 refine: with the refine off the split-FP32 sums stand for
     every row; with it on, exactly the rows whose error scale G exceeds
     |a| (or that lie far from their tile centre, G = inf) change, and
     those rows then agree with the CPU path to the FP64 tolerance; the
-    others are bit-identical."""
-    s = inputs.collision_snapshots(1, 24000, 24000, seed=8)
+    others are bit-identical.  Both routes: a set with many listed rows
+    (tiles of 128 rows) and sets with at most 32 (one warp per row and
+    source chunk)."""
+    if case == "tiles":
+        s = inputs.collision_snapshots(1, 24000, 24000, seed=8)
+    else:
+        s = inputs.cached("config1")
     try:
         gpu_ctx.keep_error_scale(True)
         gpu_ctx.set_refine(0.0)
@@ -342,6 +348,7 @@ def test_refine_recomputes_listed_rows_in_fp64(gpu_ctx):
     amag = np.sqrt(off[0] ** 2 + off[1] ** 2 + off[2] ** 2)
     listed = G > amag
     assert nref == int(listed.sum()) and nref > 0
+    assert (nref > 32) == (case == "tiles"), nref
     same = np.all([np.equal(a, b) for a, b in zip(on, off)], axis=0)
     assert np.all(same[~listed])
     rows = np.nonzero(listed)[0].astype(np.int32)
