@@ -765,7 +765,8 @@ __global__ void __launch_bounds__((W + 1) * 32) k_f32split(ComputeArgs a)
 }
 
 // name, consumer warps W, rows per thread K, threads per row Q, j-tile TJ,
-// stages NS, Newton step, quads per far-loop sub-block FQ
+// stages NS, Newton step, quads per far-loop sub-block FQ.  (Two far
+// sub-blocks per loop iteration were measured slower: 1M 511.7 vs 488.7 ms.)
 #define SG_F32_VARIANTS(X)                                              \
     X(12, 2, 1, 256, 7, false, 4, "f32split_w12_k2_q1_tj256_ns7")        \
     X(15, 2, 1, 256, 4, false, 4, "f32split_w15_k2_q1_tj256")            \
@@ -795,15 +796,21 @@ const VariantInfo &f32_variant_info(int v) { return kF32Variants[v]; }
 const void *f32_kernel(int v) { return kF32Kernels[v]; }
 int f32_smem_bytes(int v) { return kF32Smem[v]; }
 
-// Opt in to more than 48 KB of dynamic shared memory (once per variant).
+// Opt in to more than 48 KB of dynamic shared memory (once per variant and
+// device; the attribute belongs to the device's context).
 cudaError_t f32_prepare(int v)
 {
-    static bool done[kNF32] = {};
+    constexpr int MAXDEV = 64;
+    static std::atomic<bool> done[MAXDEV][kNF32];
     if (v < 0 || v >= kNF32) return cudaErrorInvalidValue;
-    if (done[v]) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kF32Kernels[v], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kF32Smem[v]);
-    if (e == cudaSuccess) done[v] = true;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const bool track = dev >= 0 && dev < MAXDEV;
+    if (track && done[dev][v].load(std::memory_order_acquire)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kF32Kernels[v], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kF32Smem[v]);
+    if (e == cudaSuccess && track) done[dev][v].store(true, std::memory_order_release);
     return e;
 }
 
