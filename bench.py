@@ -84,6 +84,10 @@ def parse():
     p.add_argument("--phases", action="store_true",
                    help="load the diagnostic build (python -m starsmasher_b200.build --phases) and "
                         "report the split-FP32 kernel's cycles per phase over 2 extra calls")
+    p.add_argument("--parallel", default="auto", choices=["auto", "rowsplit", "setshard"],
+                   help="multi-rank decomposition; auto: the reference's row split for one set, "
+                        "whole sets per rank for batches.  rowsplit/setshard also force the "
+                        "multi-rank path (NCCL) with a single rank, to exercise it on one GPU")
     p.add_argument("--tree-thetas", default="0.3,0.5",
                    help="single-set workloads: opening angles of the Barnes-Hut tree "
                         "section ('' skips it); accuracy against the FP64 kernel")
@@ -450,7 +454,16 @@ def main():
         os.environ["SPHGRAV_B200_BUILD"] = "phases"
     from starsmasher_b200 import Context, api, launch_count, multirank
 
-    if world > 1:
+    # the multi-rank code path: several ranks, or one rank when forced
+    dist_mode = world > 1 or args.parallel != "auto"
+    if dist_mode:
+        if "MASTER_ADDR" not in os.environ:  # one rank outside torchrun
+            import socket
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                port = sk.getsockname()[1]
+            os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port),
+                               "RANK": "0", "WORLD_SIZE": "1", "LOCAL_RANK": "0"})
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
@@ -487,12 +500,14 @@ def main():
             ctx.forces_device(n, *X, *outs, W=W, nkernel=args.nkernel, precision=precision)
 
     # ----------------------------------------------------- the step
-    if world == 1:
+    rowsplit = dist_mode and ((not batched and args.parallel != "setshard")
+                              or args.parallel == "rowsplit")
+    if not dist_mode:
         mode = "single GPU"
 
         def step(precision):
             gravity(precision)
-    elif not batched:
+    elif rowsplit:
         # the reference's gravity row split: this rank owns rows [lo, hi)
         lo, hi = multirank.gpu_row_range(n, world, rank)
         own = torch.stack([t[lo:hi] for t in X]).contiguous()
@@ -529,7 +544,7 @@ def main():
     torch.cuda.synchronize()
     acc_first_call = None
     calls = 0
-    if args.graph and world == 1:
+    if args.graph and not dist_mode:
         ctx.kick_reset(0)
         with ctx.capture() as cap:
             ctx.kick_device(n, X[0], X[1], X[2], sigma, kick_seed)
@@ -555,7 +570,7 @@ def main():
         torch.cuda.synchronize()
 
     def barrier():
-        if world > 1:
+        if dist_mode:
             dist.barrier()
 
     # ------------------------------------------------------- timed region
@@ -572,13 +587,13 @@ def main():
     clk = clocks.stop()
     kern_ms, kern_n = ctx.profile_read()
     ctx.profile_enable(False)
-    if world > 1:
+    if dist_mode:
         t = torch.tensor([ms_per_step], dtype=torch.float64, device=f"cuda:{device}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_per_step = float(t.item())
     value = pairs / (ms_per_step * 1e-3) / 1e9
-    refined = ctx.last_refine_rows() if world == 1 else None
-    res_f32 = [o.cpu().numpy() for o in outs] if world == 1 else None
+    refined = ctx.last_refine_rows() if not dist_mode else None
+    res_f32 = [o.cpu().numpy() for o in outs] if not dist_mode else None
     graph_info = None
     if graph is not None:
         calls += args.steps
@@ -591,7 +606,7 @@ def main():
 
     # ------------------------------------- batched vs one call per set
     batch_cmp = None
-    if world == 1 and batched and not args.no_separate:
+    if not dist_mode and batched and not args.no_separate:
         def separate(prec):
             for s in range(ws.nsets):
                 a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
@@ -612,7 +627,7 @@ def main():
     fp64 = None
     acc = None
     res64 = None
-    if world == 1 and not args.no_fp64:
+    if not dist_mode and not args.no_fp64:
         step("fp64")
         torch.cuda.synchronize()
         ms64 = timer.run(lambda: step("fp64"), 2)
@@ -631,7 +646,7 @@ def main():
     # ------------------------------------- Barnes-Hut tree (approximate)
     tree = None
     thetas = [float(v) for v in args.tree_thetas.split(",") if v.strip()]
-    if world == 1 and not batched and thetas and res64 is not None:
+    if not dist_mode and not batched and thetas and res64 is not None:
         tree = {"what": "SPHGRAV_TREE: octree, quadrupole nodes, FP64 softened pairs; "
                         "approximate, error set by theta (not the direct-sum metric)",
                 "time": "whole call, device arrays (build syncs once per 4 tree levels)",
@@ -683,7 +698,7 @@ def main():
     # ----------------------------------------------------------------- e2e
     e2e = None
     if not args.no_e2e:
-        if world > 1 and not batched:
+        if rowsplit:
             # host arrays: this rank's rows in pinned memory, copied in every
             # step; the gathered result read back every step
             own_h = torch.stack([torch.as_tensor(a[lo:hi]) for a in
@@ -714,14 +729,14 @@ def main():
                 api.lasthalf_grav_forces(n, gx, gy, gz, gp)
             how = "firsthalf_grav_forces_/lasthalf_grav_forces_ (Fortran C-ABI, host arrays)"
             h2d, d2h = 5 * 8 * n, 4 * 8 * n
-        if world == 1 or not batched:
+        if not dist_mode or rowsplit:
             e2e_step()
             barrier()
             t0 = time.perf_counter()
             for _ in range(args.steps):
                 e2e_step()
             t_e2e = time.perf_counter() - t0
-            if world > 1:
+            if dist_mode:
                 t = torch.tensor([t_e2e], dtype=torch.float64, device=f"cuda:{device}")
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
                 t_e2e = float(t.item())
@@ -731,7 +746,7 @@ def main():
 
     # -------------------------------- config4 / config5 sections (1 GPU)
     extras = {}
-    if world == 1 and args.workload == "config3" and not args.no_extras:
+    if not dist_mode and args.workload == "config3" and not args.no_extras:
         extras["config4_batched"] = config4_section(torch, ctx, timer, device, args)
         extras["config5_graph_sweep"] = config5_section(torch, ctx, timer, stream, device, args)
         for name in ("config1", "config2"):
@@ -751,7 +766,7 @@ def main():
 
     # -------------------------------------------------------- CPU baseline
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and not dist_mode and not args.no_cpu_baseline:
         cpu = cpu_baseline(ws, args.cpu_seconds)
 
     if rank == 0:
@@ -782,7 +797,7 @@ def main():
         line.update(extras)
         print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
+    if dist_mode:
         dist.destroy_process_group()
 
 
