@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <set>
 #include <string>
 #include <thread>
@@ -43,7 +44,10 @@ const VariantInfo &variant_info(int precision, int v)
 }
 int variant_occupancy(int precision, int v)
 {
+    // contexts on different host threads may ask at once
+    static std::mutex mu;
     static std::map<std::pair<int, int>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
     auto key = std::make_pair(precision, v);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
