@@ -44,6 +44,8 @@ sys.path.insert(0, ROOT)
 METRIC = "G pair-interactions/s: split-FP32 vs plain FP64 GPU at <=1e-6 rel accel error"
 UNIT = "G pair-interactions/s"
 FLOPS_PER_PAIR = 20  # far-field acc + pot convention (FMA = 2, rsqrt = 1)
+FP64_INSTR_PER_PAIR = 18  # FP64 pipe instructions per far pair of the FP64 kernel
+F32_LANE_OPS_PER_PAIR = 13  # FMA-pipe lane-ops per far pair of the split-FP32 kernel
 
 
 def parse():
@@ -641,7 +643,15 @@ def main():
                 "roofline": {"bound": "fp64-fma", "achieved": ach64, "peak": peak64, "unit": "TFLOP/s",
                              "frac": ach64 / peak64, "flops_per_pair": FLOPS_PER_PAIR,
                              "time": "whole step (preparation included)",
-                             "peak_source": "measured in-run: DFMA throughput probe on this GPU, best of 3"}}
+                             "peak_source": "measured in-run: DFMA throughput probe on this GPU, best of 3",
+                             # the kernel issues 18 FP64 instructions per far pair
+                             # (its 1/r takes 5 after the rsqrt seed), so the
+                             # FP64 pipe bounds it at peak/2 lanes/18 pairs
+                             "fp64_instructions_per_far_pair": FP64_INSTR_PER_PAIR,
+                             "instruction_bound": peak64 / 2 * 1e3 / FP64_INSTR_PER_PAIR,
+                             "frac_of_instruction_bound":
+                                 v64 / (peak64 / 2 * 1e3 / FP64_INSTR_PER_PAIR),
+                             "instruction_bound_unit": UNIT}}
 
     # ------------------------------------- Barnes-Hut tree (approximate)
     tree = None
@@ -690,6 +700,11 @@ def main():
             traffic = json.load(f).get("dram_bytes_per_launch")
     roofline = {"bound": "fp32-fma", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic,
+                # 13 FMA-pipe lane-ops per far pair against 20 counted flops:
+                # the kernel can reach at most 20 / 26 of the FMA peak
+                "fma_lane_ops_per_pair": F32_LANE_OPS_PER_PAIR,
+                "frac_cap": FLOPS_PER_PAIR / (2 * F32_LANE_OPS_PER_PAIR),
+                "frac_of_cap": achieved / peak / (FLOPS_PER_PAIR / (2 * F32_LANE_OPS_PER_PAIR)),
                 "kernel_ms_per_launch": kernel_ms, "flops_per_pair": FLOPS_PER_PAIR,
                 "peak_source": "measured in-run: packed-FFMA throughput probe on this GPU, best of 3 "
                                "(MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
