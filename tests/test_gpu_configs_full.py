@@ -42,13 +42,13 @@ def _dev(a):
     return _torch().as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()
 
 
-def _run(ctx, ws, X, precision):
+def _run(ctx, ws, X, precision, nkernel=0):
     t = _torch()
     outs = [t.empty(ws.n, dtype=t.float64, device="cuda") for _ in range(4)]
     if ws.nsets > 1:
-        ctx.batch_forces_device(ws.offsets, *X, *outs, nkernel=0, precision=precision)
+        ctx.batch_forces_device(ws.offsets, *X, *outs, nkernel=nkernel, precision=precision)
     else:
-        ctx.forces_device(ws.n, *X, *outs, nkernel=0, precision=precision)
+        ctx.forces_device(ws.n, *X, *outs, nkernel=nkernel, precision=precision)
     ctx.sync()
     return [o.cpu().numpy() for o in outs]
 
@@ -79,14 +79,14 @@ def _abs_term_sum(ws, rows):
     return out
 
 
-def _oracle_on_rows(ws, rows):
+def _oracle_on_rows(ws, rows, nkernel=0):
     """oracle.rows for global row indices (any sets): (ax, ay, az, pot)."""
     out = [np.zeros(len(rows)) for _ in range(4)]
     setid = np.searchsorted(ws.offsets, rows, side="right") - 1
     for s in np.unique(setid):
         a, b = int(ws.offsets[s]), int(ws.offsets[s + 1])
         k = np.nonzero(setid == s)[0]
-        r = oracle.rows(ws.x[a:b], ws.y[a:b], ws.z[a:b], ws.m[a:b], ws.range2[a:b], 0,
+        r = oracle.rows(ws.x[a:b], ws.y[a:b], ws.z[a:b], ws.m[a:b], ws.range2[a:b], nkernel,
                         row_idx=(rows[k] - a).astype(np.int32))
         for q in range(4):
             out[q][k] = r[q]
@@ -230,3 +230,26 @@ def test_config5_graph_sweep_first_and_last_call(ctx):
             print(f"config5 call {call} f32split vs fp64, all rows", r)
             assert r["acc_max"] <= F32_TOL and r["pot_max"] <= F32_TOL, r
         graph.close()
+
+
+@pytest.mark.parametrize("nkernel", [1, 2])
+def test_config2_wendland_kernels_against_the_cpu_path(ctx, nkernel):
+    """The two-star collision with the Wendland C6 (1) and C4 (2) softening
+    kernels (cpu_grav.f:210-248, :321-355), whose polynomials cancel hardest
+    near q = 1: 4,096 seeded rows and the 64 smallest |a| against the
+    oracle, and split-FP32 against the FP64 kernel on every row."""
+    ws = inputs.cached("config2")
+    X = [_dev(a) for a in (ws.x, ws.y, ws.z, ws.m, ws.range2)]
+    r64 = _run(ctx, ws, X, "fp64", nkernel)
+    r32 = _run(ctx, ws, X, "f32split", nkernel)
+    amag = _amag(r64)
+    median_a = float(np.median(amag))
+    rng = np.random.default_rng(20 + nkernel)
+    seeded, small = _rows_for_set(0, ws.n, amag, rng, 4096, 64)
+    for rows, allow in ((seeded, False), (small, True)):
+        ref = _oracle_on_rows(ws, rows, nkernel)
+        abs_sum = _abs_term_sum(ws, rows) if allow else None
+        _check_rows(r64, ref, rows, median_a, FP64_TOL, f"nkernel {nkernel} fp64", abs_sum)
+        _check_rows(r32, ref, rows, median_a, F32_TOL, f"nkernel {nkernel} f32split")
+    _check_rows(r32, r64, np.arange(ws.n), median_a, F32_TOL, f"nkernel {nkernel} f32 vs fp64")
+
