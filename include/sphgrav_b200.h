@@ -196,8 +196,10 @@ int sphgrav_kick_reset(sphgrav_ctx *ctx, unsigned long long c);
  * Inside the capture only *_device entry points may be called, and each of
  * them must have been called once before with the same sizes, so that every
  * buffer already exists.  The graph bakes in the context's work plan and
- * buffer addresses: after any later call on the context that changes them
- * (other sizes, precision or variant) or after sphgrav_destroy,
+ * buffer addresses, and the settings in force (FP64 band, refine threshold,
+ * error-scale keeping, theta): after any later call on the context that
+ * changes them (other sizes, precision or variant, or a new value of one of
+ * those settings) or after sphgrav_destroy,
  * sphgrav_graph_launch refuses with SPHGRAV_ERR_PROTOCOL and the graph must
  * be captured again.  Calls with the captured sizes may interleave with
  * replays. */

@@ -1503,8 +1503,9 @@ int sphgrav_graph_launch(sphgrav_graph *G, int repeats)
     if (!G->ctx) return set_err(SPHGRAV_ERR_PROTOCOL, "the graph's context was destroyed");
     if (G->ctx->epoch != G->epoch)
         return set_err(SPHGRAV_ERR_PROTOCOL,
-                       "the context's work plan or buffers changed after this graph was captured "
-                       "(a call with other sizes, precision or variant); capture it again");
+                       "the context's work plan, buffers or settings changed after this graph was "
+                       "captured (a call with other sizes, precision or variant, or a new FP64 "
+                       "band, refine threshold, error-scale setting or theta); capture it again");
     for (int r = 0; r < repeats; r++) {
         CUDA_TRY(cudaGraphLaunch(G->exec, G->stream));
         ++g_launches;
@@ -1641,6 +1642,8 @@ int sphgrav_set_fp64_band(sphgrav_ctx *c, double factor)
     if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
     if (!(factor >= 1.0 && factor <= 16.0))
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "fp64 band factor %g outside [1, 16]", factor);
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change the FP64 band during capture");
+    if (factor != c->fp64_band) ++c->epoch;  // captured graphs hold the old band
     c->fp64_band = factor;
     return SPHGRAV_OK;
 }
@@ -1651,6 +1654,7 @@ int sphgrav_set_refine(sphgrav_ctx *c, double threshold)
     if (!(threshold >= 0.0 && threshold <= 1e6))
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "refine threshold %g outside [0, 1e6]", threshold);
     if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change the refine test during capture");
+    if (threshold != c->refine_T) ++c->epoch;  // captured graphs hold the old test
     c->refine_T = threshold;
     return SPHGRAV_OK;
 }
@@ -1674,6 +1678,7 @@ int sphgrav_keep_error_scale(sphgrav_ctx *c, int on)
 {
     if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
     if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change this during capture");
+    if ((on != 0) != c->keep_scale) ++c->epoch;  // captured graphs write (or not) the scale
     c->keep_scale = on != 0;
     if (!c->keep_scale) c->scale_n = 0;
     return SPHGRAV_OK;
@@ -1823,6 +1828,8 @@ int sphgrav_set_theta(sphgrav_ctx *c, double theta)
     if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
     if (!(theta >= 0.0 && theta <= 2.0))
         return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "theta must be in [0, 2] (got %g)", theta);
+    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change theta during capture");
+    if (theta != c->theta) ++c->epoch;  // captured tree graphs hold the old angle
     c->theta = theta;
     return SPHGRAV_OK;
 }

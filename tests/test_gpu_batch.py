@@ -288,3 +288,37 @@ def test_graph_destroyed_during_another_capture(gpu_ctx):
     for o, w in zip(outs, want):
         assert np.array_equal(o.cpu().numpy(), w)
 
+
+def test_graph_refuses_replay_after_a_setting_changes():
+    """Settings a captured graph bakes in (the FP64 band, the refine
+    threshold) cannot change under it: changing one invalidates the graph,
+    and setting the same value again does not."""
+    from starsmasher_b200 import Context, _lib
+    t = _t()
+    b = inputs.batch_models(2, 500, 1500, seed=77)
+    X = [dev(a) for a in (b.x, b.y, b.z, b.m, b.range2)]
+    outs = [t.zeros(b.n, dtype=t.float64, device="cuda") for _ in range(4)]
+    ctx = Context(0)
+    try:
+        for change in (lambda c: c.set_fp64_band(1.5), lambda c: c.set_refine(2.0)):
+            ctx.set_fp64_band(1.0)
+            ctx.set_refine(1.0)
+            ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")
+            ctx.sync()
+            with ctx.capture() as cap:
+                ctx.batch_forces_device(b.offsets, *X, *outs, precision="f32split")
+            ctx.set_fp64_band(1.0)  # unchanged: the graph stays valid
+            assert cap.graph.valid
+            cap.graph.launch(1)
+            change(ctx)
+            assert not cap.graph.valid
+            with pytest.raises(_lib.SphgravError) as e:
+                cap.graph.launch(1)
+            assert e.value.status == _lib.ERR_PROTOCOL
+            cap.graph.close()
+        ctx.sync()
+    finally:
+        ctx.set_fp64_band(1.0)
+        ctx.set_refine(1.0)
+        ctx.close()
+
