@@ -1083,12 +1083,9 @@ static int upload_inputs(sphgrav_ctx *c, int n, const double *x, const double *y
     for (int a = 0; a < 5; a++) dst[a] = h + (size_t)a * n;
     copy_arrays(5, n, dst, 0, src, 0);
     const size_t cap = c->io_cap;
-    if (n > 0) {
-        // the device buffer holds 5 arrays of io_cap; copy each
-        for (int a = 0; a < 5; a++)
-            CUDA_TRY(cudaMemcpyAsync(c->in.p + a * cap, h + (size_t)a * n, sizeof(double) * n,
-                                     cudaMemcpyHostToDevice, c->stream));
-    }
+    if (n > 0)  // the device buffer holds 5 arrays of io_cap: one strided copy
+        CUDA_TRY(cudaMemcpy2DAsync(c->in.p, sizeof(double) * cap, h, sizeof(double) * n,
+                                   sizeof(double) * n, 5, cudaMemcpyHostToDevice, c->stream));
     in.x = c->in.p;
     in.y = in.x + cap;
     in.z = in.y + cap;
@@ -1300,10 +1297,9 @@ int sphgrav_batch_forces(sphgrav_ctx *c, int nsets, const int *offsets, const do
     TRY(run_device(c, offs, true, 0, 0, in, out, c->wdev.p, nkernel, precision));
     TRY(ensure_pinned(c, c->h_out, sizeof(double) * (4 * (size_t)n + nsets)));
     double *h = (double *)c->h_out.p;
-    if (n > 0)
-        for (int q = 0; q < 4; q++)
-            CUDA_TRY(cudaMemcpyAsync(h + (size_t)q * n, c->out.p + (size_t)q * c->io_cap,
-                                     sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    if (n > 0)  // 4 output arrays of io_cap: one strided copy
+        CUDA_TRY(cudaMemcpy2DAsync(h, sizeof(double) * n, c->out.p, sizeof(double) * c->io_cap,
+                                   sizeof(double) * n, 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaMemcpyAsync(h + 4 * (size_t)n, c->wdev.p, sizeof(double) * nsets,
                              cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1338,10 +1334,10 @@ int sphgrav_firsthalf(sphgrav_ctx *c, int n, int i_begin, int ni, const double *
     TRY(run_device(c, offs, full, i_begin, ni, in, out, nullptr, nkernel, precision));
     TRY(ensure_pinned(c, c->h_out, sizeof(double) * 4 * (size_t)std::max(ni, 1)));
     double *h = (double *)c->h_out.p;
-    if (ni > 0)
-        for (int q = 0; q < 4; q++)
-            CUDA_TRY(cudaMemcpyAsync(h + (size_t)q * ni, c->out.p + (size_t)q * c->io_cap + i_begin,
-                                     sizeof(double) * ni, cudaMemcpyDeviceToHost, c->stream));
+    if (ni > 0)  // the row slice of the 4 output arrays: one strided copy
+        CUDA_TRY(cudaMemcpy2DAsync(h, sizeof(double) * ni, c->out.p + i_begin,
+                                   sizeof(double) * c->io_cap, sizeof(double) * ni, 4,
+                                   cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaMemcpyAsync(c->h_err.p, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
     CUDA_TRY(cudaEventRecord(c->ev_done, c->stream));
