@@ -375,3 +375,21 @@ def test_fp64_band_rejects_bad_values(gpu_ctx):
         with pytest.raises(_lib.SphgravError) as e:
             gpu_ctx.set_fp64_band(bad)
         assert e.value.status == _lib.ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("shift", [(1.0e4, -2.0e4, 5.0e3), (3.0e6, 0.0, -1.0e6)])
+def test_model_far_from_the_origin(gpu_ctx, shift):
+    """A star model displaced far from the coordinate origin (a collision's
+    stars sit at large separations): both kernels still agree with the CPU
+    path on the same (displaced) inputs.  The split kernel forms separations
+    from hi + lo position pairs relative to each tile's centre, so the
+    displacement costs it nothing; the FP64 kernel rounds x_j - x_i as the
+    CPU path does."""
+    s = inputs.single_polytrope(6000, 1.5, seed=91)
+    x, y, z = s.x + shift[0], s.y + shift[1], s.z + shift[2]
+    tri = oracle.triangle(x, y, z, s.m, s.range2, 0)
+    for precision, tol in (("fp64", FP64_TOL), ("f32split", F32_TOL)):
+        got = gpu_ctx.forces(x, y, z, s.m, s.range2, 0, precision)
+        r = err_report(*got, *tri)
+        print("displaced by", shift, precision, r)
+        assert r["acc_max"] <= tol and r["pot_max"] <= tol, (precision, r)
