@@ -238,14 +238,14 @@ __device__ __noinline__ void near_eval(const SortedF64 D, int nkernel, int jbase
 }
 
 // Pairs with r < band * max(H_i, H_j) take the FP64 path (ComputeArgs::band2 =
-// band^2, >= 1; default band 2).  Below H that is the softened near field
-// (reference polynomials, which cancel in FP32); between H and band*H it is
-// the Newtonian term in FP64: these are the largest far-field terms, and in
-// FP32 their rounding alone sets a ~1e-6 floor on the relative error of a
-// particle whose acceleration cancels (|a| ~ 0.05 median), while at band 2
-// they are only ~1e-3 of all pairs at N=1M.  Scaling H^2 by band2 only moves
-// pairs between two correct evaluations; with band2 >= 1 every r < H pair
-// stays on the FP64 path.
+// band^2, >= 1; default band 1, sphgrav_set_fp64_band).  Below H that is the
+// softened near field (reference polynomials, which cancel in FP32); a band
+// above 1 also moves the Newtonian terms between H and band*H, the largest
+// far-field terms, to FP64.  The rows whose FP32 sums are ill-conditioned
+// anyway (acceleration that cancels) are recomputed in FP64 by the refine,
+// which is why band 1 suffices.  Scaling H^2 by band2 only moves pairs
+// between two correct evaluations; with band2 >= 1 every r < H pair stays on
+// the FP64 path.
 
 // Shared-memory layout of one CTA (dynamic shared memory, byte offsets).
 template <int W, int K, int Q, int TJ, int NS>
