@@ -358,8 +358,9 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     //                                 768-row tiles leave more rows beyond
     //                                 8 H of their centre for the FP64
     //                                 refine: 2,357 rows, whole call 37.5 ms)
-    //   15..16   W15K1Q2             (32K: 0.791 vs 0.827; 64K: 2.52 vs 2.58)
-    //   13..14   W12K1Q4, 7 stages   (8K: 0.135 vs 0.142; 16K: 0.299 vs 0.298)
+    //   14..16   W15K1Q2             (16K: 0.302 vs 0.307 for W12K1Q4; 32K: 0.791
+    //                                 vs 0.827; 64K: 2.52 vs 2.58)
+    //   13       W12K1Q4, 7 stages   (8K: 0.135 vs 0.142)
     //   <= 12    W8K1Q4              (4K: 75 vs 72 G pairs/s)
     // Twelve consumer warps put the same number of consumers on every SMSP;
     // all without the Newton step on rsqrt.approx: in FP32 the step's own
@@ -368,7 +369,7 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     // workload) and it is 3 of 16 FMA-pipe lane-ops per pair.
     if (b >= 20 || (batch && b >= 18)) return 0;
     if (b >= 17 || (batch && b >= 15)) return 2;
-    if (b >= 15) return 3;
+    if (b >= 14) return 3;
     if (b >= 13) return 5;
     return 4;
 }
