@@ -44,15 +44,15 @@
 //     the tile sum in the far loop.  Per row the kernel also keeps G^2, the
 //     sum over tiles of |FP32 tile sum|^2 (the scale of the FP32 rounding
 //     error), for the FP64 refine of ill-conditioned rows (sg_refine.cu).
-//   * pairs with r < 2 max(H_i, H_j) are masked out of the FP32 sums by the
-//     checked loop, flagged in per-thread bit masks, and evaluated after the
-//     tile's FP32 loop in FP64 with the CPU-path formulas, one pair per lane
-//     of the warp (near_eval), then folded into the same accumulators: below
-//     H the softened near field, whose reference polynomials cancel by up to
-//     ~1e3 near q = 1, and between H and 2H the largest Newtonian terms (see
-//     ComputeArgs::band2).  A warp skips the per-pair test (the far loop)
-//     for a tile when the bounding boxes of its rows and of the tile are
-//     farther apart than 2 max(H) of both.
+//   * pairs with r < band max(H_i, H_j) (band 1 by default) are masked out
+//     of the FP32 sums by the checked loop, flagged in per-thread bit masks,
+//     and evaluated after the tile's FP32 loop in FP64 with the CPU-path
+//     formulas, one pair per lane of the warp (near_eval), then folded into
+//     the same accumulators: the softened near field, whose reference
+//     polynomials cancel by up to ~1e4 near q = 1 (a larger band also moves
+//     the largest Newtonian terms, see ComputeArgs::band2).  A warp skips the
+//     per-pair test (the far loop) for a tile when the bounding boxes of its
+//     rows and of the tile are farther apart than band max(H) of both.
 //   * per (row, j-chunk) results leave the CTA as FP64 partial sums merged in
 //     chunk order (k_merge).
 // Reference kernel replaced: dev_compute_forces / dev_force_ij_nkernel*
