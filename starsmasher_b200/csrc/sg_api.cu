@@ -358,9 +358,11 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     //                                 768-row tiles leave more rows beyond
     //                                 8 H of their centre for the FP64
     //                                 refine: 2,357 rows, whole call 37.5 ms)
-    //   14..16   W15K1Q2             (16K: 0.302 vs 0.307 for W12K1Q4; 32K: 0.791
-    //                                 vs 0.827; 64K: 2.52 vs 2.58)
-    //   13       W12K1Q4, 7 stages   (8K: 0.135 vs 0.142)
+    //   15..16   W15K1Q2             (32K: 0.791 vs 0.827; 64K: 2.52 vs 2.58)
+    //   13..14   W12K1Q4, 7 stages   (8K: 0.135 vs 0.142; 16K: 0.307 vs 0.302 for
+    //                                 W15K1Q2, whose 240-row tiles leave 69 rows
+    //                                 for the FP64 refine against 22: whole call
+    //                                 0.51 vs 0.63 ms)
     //   <= 12    W8K1Q4              (4K: 75 vs 72 G pairs/s)
     // Twelve consumer warps put the same number of consumers on every SMSP;
     // all without the Newton step on rsqrt.approx: in FP32 the step's own
@@ -369,7 +371,7 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     // workload) and it is 3 of 16 FMA-pipe lane-ops per pair.
     if (b >= 20 || (batch && b >= 18)) return 0;
     if (b >= 17 || (batch && b >= 15)) return 2;
-    if (b >= 14) return 3;
+    if (b >= 15) return 3;
     if (b >= 13) return 5;
     return 4;
 }
