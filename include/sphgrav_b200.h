@@ -299,6 +299,14 @@ unsigned long long sphgrav_launch_count(void);
 /* Work items and j-chunks of the last computation (for tests and tuning). */
 int sphgrav_last_plan_info(sphgrav_ctx *ctx, int *nitems, int *nchunks_max,
                            int *variant);
+/* The work plan a call on whole sets would use, computed on the host only
+ * (no context, no GPU needed): `resident` persistent CTAs of `variant` of
+ * `precision`.  Writes the item and partial-slot counts and, for up to `cap`
+ * items in queue order, 6 ints each: set, row tile, chunk, slot, first and
+ * end source slot of the chunk (set-local).  For tests and tuning; no
+ * counterpart in the reference. */
+int sphgrav_plan_preview(int nsets, const int *offsets, int precision, int variant, int resident,
+                         int *nitems, int *nslots, int *items, int cap);
 /* Kernel timing: while enabled, CUDA events are recorded on the context's
  * stream around every pair-sum kernel launch (not inside graph captures);
  * sphgrav_profile_read returns the summed kernel milliseconds and launch

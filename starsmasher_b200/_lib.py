@@ -83,6 +83,7 @@ SIGNATURES = {
     "sphgrav_forces_fp64_noalloc": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "sphgrav_profile_enable": (_I, [_P, _I]),
     "sphgrav_profile_read": (_I, [_P, _PD, _PI]),
+    "sphgrav_plan_preview": (_I, [_I, _PI, _I, _I, _I, _PI, _PI, _PI, _I]),
     "sphgrav_phase_read": (_I, [_P, ctypes.POINTER(ctypes.c_ulonglong), _I]),
 }
 

@@ -339,6 +339,28 @@ def launch_count() -> int:
     return int(load().sphgrav_launch_count())
 
 
+def plan_preview(offsets: Sequence[int], precision="f32split", variant: int = 0,
+                 resident: int = 148) -> dict:
+    """The work plan of a call on whole sets, computed on the host (no GPU):
+    {"nitems", "nslots", "items"}; items is an (nitems, 6) int array of
+    (set, row tile, chunk, partial slot, first source, end source) in queue
+    order, `resident` persistent CTAs."""
+    lib = load()
+    offs = np.ascontiguousarray(offsets, dtype=np.int32)
+    ni, ns = ctypes.c_int(), ctypes.c_int()
+    check(lib.sphgrav_plan_preview(len(offs) - 1, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   _prec(precision), int(variant), int(resident),
+                                   ctypes.byref(ni), ctypes.byref(ns), None, 0),
+          "sphgrav_plan_preview")
+    items = np.zeros((max(ni.value, 1), 6), dtype=np.int32)
+    check(lib.sphgrav_plan_preview(len(offs) - 1, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   _prec(precision), int(variant), int(resident),
+                                   ctypes.byref(ni), ctypes.byref(ns),
+                                   items.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ni.value),
+          "sphgrav_plan_preview")
+    return {"nitems": ni.value, "nslots": ns.value, "items": items[:ni.value]}
+
+
 # ------------------------------------------- reference-named module functions
 def gpu_init_dev(myrank: int, theta: float = 0.3) -> None:
     """gpu_init_dev(myrank, theta) of main.f:265-275: select device ``myrank``."""

@@ -377,7 +377,10 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
 }
 
 // ------------------------------------------------------------------ plan
-static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
+// The work plan of one call: host-only arithmetic (resident = persistent CTAs
+// of the variant on the device), so it also runs without a GPU
+// (sphgrav_plan_preview).
+static int build_plan(int resident, const std::vector<int> &offsets, bool full_rows, int i_lo,
                       int ni, int precision, int variant, Plan &P)
 {
     const VariantInfo &V = variant_info(precision, variant);
@@ -419,8 +422,6 @@ static int build_plan(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     P.rows_tot = (int)ioff;
     P.ntiles = (int)toff;
     P.nmeta = (int)moff;
-    const int occ = variant_occupancy(precision, variant);
-    const int resident = occ * c->sm_count;
     const int target = 4 * resident;
     // One set: items are all alike, so pick the chunk count whose item count
     // fills the last wave of persistent CTAs best (ties: fewer chunks).
@@ -544,7 +545,8 @@ static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_ro
                            "work plan changed during a graph capture; call the entry point once "
                            "with the same sizes before capturing");
         Plan P;
-        TRY(build_plan(c, offsets, full_rows, i_lo, ni, precision, variant, P));
+        TRY(build_plan(variant_occupancy(precision, variant) * c->sm_count, offsets, full_rows,
+                       i_lo, ni, precision, variant, P));
         ++c->epoch;  // graphs captured under the old plan must not replay
         TRY(ensure(c, c->sets, std::max(1, P.nsets), "sets"));
         TRY(ensure(c, c->tile_set, std::max(1, P.ntiles), "tile_set"));
@@ -1633,6 +1635,33 @@ int sphgrav_last_plan_info(sphgrav_ctx *c, int *nitems, int *nchunks_max, int *v
     if (nitems) *nitems = c->plan.nitems;
     if (nchunks_max) *nchunks_max = c->plan.nchunks_max;
     if (variant) *variant = c->plan.variant;
+    return SPHGRAV_OK;
+}
+
+int sphgrav_plan_preview(int nsets, const int *offsets, int precision, int variant, int resident,
+                         int *nitems, int *nslots, int *items, int cap)
+{
+    if (nsets <= 0 || nsets > MAX_SETS || !offsets || !nitems || !nslots || resident <= 0)
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "plan_preview: bad arguments");
+    if ((precision != SPHGRAV_FP64 && precision != SPHGRAV_F32SPLIT) || variant < 0 ||
+        variant >= variant_count(precision))
+        return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "plan_preview: unknown precision or variant");
+    std::vector<int> offs(offsets, offsets + nsets + 1);
+    if (offs[0] != 0) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "offsets[0] must be 0");
+    for (int s = 0; s < nsets; s++)
+        if (offs[s + 1] < offs[s]) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "offsets must not decrease");
+    Plan P;
+    TRY(build_plan(resident, offs, true, 0, 0, precision, variant, P));
+    *nitems = P.nitems;
+    *nslots = P.nslots;
+    if (items) {
+        const int m = std::min(cap, P.nitems);
+        for (int k = 0; k < m; k++) {
+            const WorkItem &w = P.items[k];
+            int *o = items + 6 * (size_t)k;
+            o[0] = w.set; o[1] = w.tile; o[2] = w.chunk; o[3] = w.slot; o[4] = w.jb; o[5] = w.je;
+        }
+    }
     return SPHGRAV_OK;
 }
 
