@@ -242,17 +242,6 @@ int sphgrav_set_fp64_band(sphgrav_ctx *ctx, double factor);
  * Default 1.0 (0.1-0.4% of the rows of the benchmark workloads); 0 turns the
  * refine off.  No reference counterpart. */
 int sphgrav_set_refine(sphgrav_ctx *ctx, double threshold);
-/* Split-FP32 whole-set calls: evaluate each unordered pair once and apply it
- * to both particles (on != 0), as the reference's CPU path does
- * (cpu_grav.f, the j >= i triangle): 9 FP32 lane-operations per interaction
- * instead of 13.  The mirrored terms are summed as integers at bounded
- * scales, so results stay deterministic.  Needs the FP64 refine (threshold
- * > 0); calls on a row range, FP64 calls and calls with the refine off use
- * the one-sided kernels.  Default off.  Replaying a graph captured before a
- * change returns SPHGRAV_ERR_PROTOCOL.  No counterpart in the reference's
- * GPU library. */
-int sphgrav_set_mutual(sphgrav_ctx *ctx, int on);
-int sphgrav_get_mutual(sphgrav_ctx *ctx, int *on);
 /* Rows the last split-FP32 call recomputed in FP64 (0 when the refine was
  * off or the call was not split-FP32).  Synchronises the context's stream. */
 int sphgrav_last_refine_rows(sphgrav_ctx *ctx, long long *rows);

@@ -66,8 +66,6 @@ SIGNATURES = {
     "sphgrav_force_variant": (_I, [_P, _I, _I]),
     "sphgrav_set_fp64_band": (_I, [_P, _D]),
     "sphgrav_set_refine": (_I, [_P, _D]),
-    "sphgrav_set_mutual": (_I, [_P, _I]),
-    "sphgrav_get_mutual": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
     "sphgrav_last_refine_rows": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "sphgrav_keep_error_scale": (_I, [_P, _I]),
     "sphgrav_error_scale": (_I, [_P, _I, _P]),

@@ -141,17 +141,6 @@ class Context:
         threshold * |a| (default 1.0; 0 turns the refine off)."""
         check(self._lib.sphgrav_set_refine(self._h, float(threshold)), "sphgrav_set_refine")
 
-    def set_mutual(self, on: bool = True) -> None:
-        """Split-FP32 whole-set calls: evaluate each pair once and apply it to
-        both particles (the mutual-update kernel; needs the refine on)."""
-        check(self._lib.sphgrav_set_mutual(self._h, 1 if on else 0), "sphgrav_set_mutual")
-
-    @property
-    def mutual(self) -> bool:
-        v = ctypes.c_int(0)
-        check(self._lib.sphgrav_get_mutual(self._h, ctypes.byref(v)), "sphgrav_get_mutual")
-        return bool(v.value)
-
     def last_refine_rows(self) -> int:
         """Rows the last split-FP32 call recomputed in FP64 (synchronises)."""
         v = ctypes.c_longlong(0)

@@ -24,8 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = ["sg_prep.cu", "sg_f64.cu", "sg_f32.cu", "sg_f32sym.cu", "sg_refine.cu", "sg_tree.cu",
-           "sg_api.cu", "sg_noalloc.cu"]
+SOURCES = ["sg_prep.cu", "sg_f64.cu", "sg_f32.cu", "sg_refine.cu", "sg_tree.cu", "sg_api.cu",
+           "sg_noalloc.cu"]
 SO_NAME = "libsphgrav_b200.so"
 PHASES_SO_NAME = "libsphgrav_b200_phases.so"
 A_NAME = "libSPHgrav.a"

@@ -242,12 +242,6 @@ struct sphgrav_ctx {
 
     // kernel timing (sphgrav_profile_*)
     double fp64_band = 1.0;  // split-FP32: FP64 for r < fp64_band * max(H)
-    // split-FP32 whole-set calls: the mutual-update kernel (each pair once,
-    // applied to both particles) when on; it needs the FP64 refine
-    bool mutual = false;
-    DBuf<long long> jacc;    // [9][pcap] integer sums of the mirrored terms
-    DBuf<int> jword;         // [pcap] slot exponent words
-    DBuf<double> symstats;   // [2][nsets] set mass, smallest H^2
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
@@ -332,17 +326,10 @@ static int variant_by_name(int precision, const std::string &name)
     return -1;
 }
 
-static int mutual_first() { return f32_variant_count() - sym_variant_count(); }
-static bool mutual_ok(const sphgrav_ctx *c, int precision, bool full_rows)
-{
-    return precision == SPHGRAV_F32SPLIT && full_rows && c->refine_T > 0.0;
-}
-
 static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> &offsets,
                           bool full_rows, int ni)
 {
     if (c->forced_variant[precision] >= 0) return c->forced_variant[precision];
-    if (c->mutual && mutual_ok(c, precision, full_rows)) return mutual_first();
     const int b = bucket_of(offsets, full_rows, ni);
     auto it = c->tuned[precision].find(b);
     if (it != c->tuned[precision].end()) {
@@ -496,69 +483,6 @@ static int build_plan(int resident, const std::vector<int> &offsets, bool full_r
             tile_nch[t] = std::min(TAIL_CHUNKS, set_maxch(P.sets[P.tile_set_of(t)]));
         }
     }
-    if (V.sym) {
-        // Mutual updates: row tile t sums sources from its own first slot on
-        // (from the start of the j-tile holding it; the kernel excludes the
-        // earlier slots); pairs with earlier row tiles are theirs.  Costs fall
-        // along the triangle, so the longest-first queue balances them; tiles
-        // longer than a third of a persistent CTA's share are cut into chunks.
-        if (!full_rows)
-            return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "mutual-update variants need whole sets");
-        long long total = 0;
-        for (const SetDesc &d : P.sets)
-            for (int t = 0; t < d.ntiles; t++)
-                total += (long long)std::min(P.itile, d.ni - t * P.itile) *
-                         (d.npad - (long long)t * P.itile);
-        const long long target = std::max(1ll, total / (3ll * std::max(1, resident)));
-        struct CostS { long long cost; WorkItem w; };
-        std::vector<CostS> its;
-        int slot = 0;
-        P.nchunks_max = 1;
-        for (int s = 0; s < P.nsets; s++) {
-            SetDesc &d = P.sets[s];
-            const int jtiles = (d.n + P.tj - 1) / P.tj;
-            d.nchunks = 1;
-            d.slot_off = slot;
-            for (int t = 0; t < d.ntiles; t++) {
-                const int rows = std::min(P.itile, d.ni - t * P.itile);
-                const int jt0 = (t * P.itile) / P.tj;  // j-tile holding the row tile's first slot
-                const int len = std::max(1, jtiles - jt0);
-                const long long cost = (long long)rows * (len * (long long)P.tj);
-                const int maxch =
-                    std::max(1, std::min(len, (int)((long long)len * P.tj / kMinChunkJ)));
-                const int nch =
-                    (int)std::max(1ll, std::min<long long>(maxch, (cost + target - 1) / target));
-                P.tile_slots.push_back({slot, nch});
-                d.nchunks = std::max(d.nchunks, nch);
-                for (int ch = 0; ch < nch; ch++) {
-                    WorkItem w;
-                    memset(&w, 0, sizeof(w));
-                    w.set = s;
-                    w.tile = t;
-                    w.chunk = ch;
-                    w.slot = slot + ch;
-                    w.jb = (jt0 + (int)((long long)len * ch / nch)) * P.tj;
-                    w.je = (jt0 + (int)((long long)len * (ch + 1) / nch)) * P.tj;
-                    its.push_back({(long long)rows * (w.je - w.jb), w});
-                }
-                slot += nch;
-            }
-            P.nchunks_max = std::max(P.nchunks_max, d.nchunks);
-            for (int t = 0; t < d.ntiles; t++) P.tile_set.push_back(s);
-            for (int r = 0; r < d.npad / META_J; r++) P.meta_set.push_back(s);
-        }
-        std::stable_sort(its.begin(), its.end(),
-                         [](const CostS &a, const CostS &b) { return a.cost > b.cost; });
-        for (auto &it : its) P.items.push_back(it.w);
-        P.nitems = (int)P.items.size();
-        P.nslots = slot;
-        P.grid = std::max(1, std::min(P.nitems, resident));
-        const int setbits = ceil_log2(std::max(1, P.nsets));
-        P.bits = std::min(21, (64 - setbits) / 3);
-        P.end_bit = 3 * P.bits + setbits;
-        P.valid = true;
-        return SPHGRAV_OK;
-    }
     int slot = 0;
     P.nchunks_max = 1;
     struct Cost { long long cost; WorkItem w; };
@@ -686,14 +610,6 @@ static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_ro
         TRY(ensure(c, c->rlpart, 4 * (size_t)REFINE_LIGHT_CAP, "refine row-chunk partials"));
         TRY(ensure(c, c->rnlight, 1, "refine row-chunk items"));
         if (c->keep_scale) TRY(ensure(c, c->scale, std::max(1, P.ntot), "error scale"));
-    }
-    if (P.precision == SPHGRAV_F32SPLIT && variant_info(P.precision, P.variant).sym) {
-        if (!(c->refine_T > 0.0))
-            return set_err(SPHGRAV_ERR_INVALID_ARGUMENT,
-                           "mutual-update variants need the FP64 refine (threshold > 0)");
-        TRY(ensure(c, c->jacc, 9 * c->pcap, "mirrored sums"));
-        TRY(ensure(c, c->jword, c->pcap, "mirrored-sum scales"));
-        TRY(ensure(c, c->symstats, 2 * (size_t)std::max(1, P.nsets), "set mass"));
     }
     const size_t sb = sort_temp_bytes(P.ntot, P.end_bit);
     TRY(ensure(c, c->sort_temp, std::max<size_t>(sb, 1), "sort temp"));
@@ -992,11 +908,6 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
                                    c->ilist.p, D, c->imeta.p, st));
     // source boxes: both kernels skip the per-pair near test on far tiles
     CUDA_TRY(launch_jmeta(c->sets.p, P.nsets, P.nmeta, c->meta_set.p, D, c->jmeta.p, st));
-    const bool mutual = precision == SPHGRAV_F32SPLIT && variant_info(precision, P.variant).sym;
-    if (mutual) {
-        CUDA_TRY(launch_sym_words(c->sets.p, P.nsets, P.max_npad, D, c->symstats.p, c->jword.p, st));
-        CUDA_TRY(cudaMemsetAsync(c->jacc.p, 0, sizeof(long long) * 9 * c->pcap, st));
-    }
     CUDA_TRY(cudaMemsetAsync(c->head.p, 0, sizeof(int), st));
     ComputeArgs a{};
     a.sets = c->sets.p;
@@ -1014,11 +925,6 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
     a.itile = P.itile;
     a.band2 = (float)(c->fp64_band * c->fp64_band);
     a.nitems_dev = nullptr;
-    if (mutual) {
-        a.jacc = c->jacc.p;
-        a.jword = c->jword.p;
-        a.jstride = c->pcap;
-    }
     const bool refine = precision == SPHGRAV_F32SPLIT && c->refine_T > 0.0;
     const bool want_g = precision == SPHGRAV_F32SPLIT && (refine || c->keep_scale);
     a.gpart = want_g ? c->gpart.p : nullptr;
@@ -1047,11 +953,6 @@ static int run_device(sphgrav_ctx *c, const std::vector<int> &offsets, bool full
         R.gpart = c->gpart.p;
         R.scale = c->keep_scale ? c->scale.p : nullptr;
         c->scale_n = c->keep_scale ? P.ntot : 0;
-    }
-    if (mutual) {
-        R.jacc = c->jacc.p;
-        R.jword = c->jword.p;
-        R.jstride = c->pcap;
     }
     if (refine) {
         R.thresh2 = c->refine_T * c->refine_T;
@@ -1659,7 +1560,6 @@ int sphgrav_autotune(sphgrav_ctx *c, int nsets, const int *offsets, const double
     for (int v = 0; v < variant_count(precision); v++) {
         const VariantInfo &V = variant_info(precision, v);
         if (precision == SPHGRAV_F32SPLIT && V.newton) continue;  // same numerics as the defaults
-        if (V.sym && !(c->mutual && mutual_ok(c, precision, true))) continue;
         c->forced_variant[precision] = v;
         int st = run_device(c, offs, true, 0, 0, in, out, nullptr, nkernel, precision);
         if (st != SPHGRAV_OK) { c->forced_variant[precision] = saved; return st; }
@@ -1773,22 +1673,6 @@ int sphgrav_set_fp64_band(sphgrav_ctx *c, double factor)
     if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change the FP64 band during capture");
     if (factor != c->fp64_band) ++c->epoch;  // captured graphs hold the old band
     c->fp64_band = factor;
-    return SPHGRAV_OK;
-}
-
-int sphgrav_set_mutual(sphgrav_ctx *c, int on)
-{
-    if (!c) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "ctx is NULL");
-    if (c->capturing) return set_err(SPHGRAV_ERR_PROTOCOL, "cannot change this during capture");
-    if ((on != 0) != c->mutual) ++c->epoch;  // captured graphs hold the old kernel
-    c->mutual = on != 0;
-    return SPHGRAV_OK;
-}
-
-int sphgrav_get_mutual(sphgrav_ctx *c, int *on)
-{
-    if (!c || !on) return set_err(SPHGRAV_ERR_INVALID_ARGUMENT, "NULL argument");
-    *on = c->mutual ? 1 : 0;
     return SPHGRAV_OK;
 }
 

@@ -61,6 +61,12 @@
 
 namespace sg {
 
+struct TileBox {
+    float lo[3], hi[3];
+    float h2max;
+    int empty;
+};
+
 template <bool NEWTON>
 struct Scales {
     // accumulated value * scale = physical value
@@ -102,6 +108,18 @@ __device__ __forceinline__ void accum2(f2 dx, f2 dy, f2 dz, f2 r2, f2 mj, f2 &ax
     ay = fma2(mr3, dy, ay);
     az = fma2(mr3, dz, az);
     pp = add2(pp, mr);
+}
+
+// Fold a packed FP32 partial into a compensated accumulator pair in shared memory.
+__device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
+{
+    float a, b;
+    upk(v, a, b);
+    float h = *hi, l = *lo;
+    ff_add(h, l, a);
+    ff_add(h, l, b);
+    *hi = h;
+    *lo = l;
 }
 
 // Near-field pair (r^2 < max H^2) in FP64, folded into the row's
@@ -773,14 +791,10 @@ static const int kF32Smem[] = {SG_F32_VARIANTS(SG_SMEM)};
 #undef SG_SMEM
 constexpr int kNF32 = sizeof(kF32Variants) / sizeof(kF32Variants[0]);
 
-// Variants kNF32 and up are the mutual-update kernels (sg_f32sym.cu).
-int f32_variant_count() { return kNF32 + sym_variant_count(); }
-const VariantInfo &f32_variant_info(int v)
-{
-    return v < kNF32 ? kF32Variants[v] : sym_variant_info(v - kNF32);
-}
-const void *f32_kernel(int v) { return v < kNF32 ? kF32Kernels[v] : sym_kernel(v - kNF32); }
-int f32_smem_bytes(int v) { return v < kNF32 ? kF32Smem[v] : sym_smem_bytes(v - kNF32); }
+int f32_variant_count() { return kNF32; }
+const VariantInfo &f32_variant_info(int v) { return kF32Variants[v]; }
+const void *f32_kernel(int v) { return kF32Kernels[v]; }
+int f32_smem_bytes(int v) { return kF32Smem[v]; }
 
 // Opt in to more than 48 KB of dynamic shared memory (once per variant and
 // device; the attribute belongs to the device's context).
@@ -788,8 +802,7 @@ cudaError_t f32_prepare(int v)
 {
     constexpr int MAXDEV = 64;
     static std::atomic<bool> done[MAXDEV][kNF32];
-    if (v >= kNF32) return sym_prepare(v - kNF32);
-    if (v < 0) return cudaErrorInvalidValue;
+    if (v < 0 || v >= kNF32) return cudaErrorInvalidValue;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -803,7 +816,6 @@ cudaError_t f32_prepare(int v)
 
 cudaError_t launch_f32(int v, int grid, const ComputeArgs &a, cudaStream_t st)
 {
-    if (v >= kNF32) return launch_sym(v - kNF32, grid, a, st);
     cudaError_t e = f32_prepare(v);
     if (e != cudaSuccess) return e;
     int idx = 0;

@@ -61,8 +61,7 @@ struct JMeta {
 // Centre of an i-tile's bounding box as float hi + lo pairs.
 struct ITileMeta {
     float chx, chy, chz, clx, cly, clz;
-    float mass;   // total mass of the tile's rows (FP32, rounded up; mutual-update bounds)
-    float h2min;  // smallest H^2 among them (rounded down)
+    float pad_[2];
 };
 
 // Error flag bits written by device code.
@@ -416,103 +415,6 @@ __device__ __forceinline__ void ff_add_d(float &hi, float &lo, double v)
     const float vl = __double2float_rn(v - (double)vh);
     ff_add(hi, lo, vh);
     lo = __fadd_rn(lo, vl);
-}
-
-// Fold a packed FP32 partial into a compensated accumulator pair in shared memory.
-__device__ __forceinline__ void fold(float *hi, float *lo, f2 v)
-{
-    float a, b;
-    upk(v, a, b);
-    float h = *hi, l = *lo;
-    ff_add(h, l, a);
-    ff_add(h, l, b);
-    *hi = h;
-    *lo = l;
-}
-
-// Bounding box of a staged j-tile relative to the i-tile centre, and its
-// largest (band H)^2 (split-FP32 kernels' per-warp far test).
-struct TileBox {
-    float lo[3], hi[3];
-    float h2max;
-    int empty;
-};
-
-// ------------------------------------- mutual updates: fixed-point sums
-// The split-FP32 kernel with mutual updates (sg_f32sym.cu) evaluates each
-// unordered pair once and adds the mirrored term, -m_i f(r) dr and m_i phi,
-// to the source particle j.  Those terms come from many CTAs, so they are
-// summed as integers (exact and order-free, hence deterministic):
-//   * inside a CTA, per staged j-tile, in int64 at a tile-local scale
-//     2^e (e = SYM_LOCAL_BITS - ceil(log2 B_loc));
-//   * across CTAs, per sorted slot, as two int64 words at the slot's scale
-//     2^E (E = SYM_GLOBAL_BITS - ceil(log2 B)): hi * 2^SYM_LO_BITS + lo, with
-//     0 <= lo < 2^SYM_LO_BITS per contribution, so neither word overflows.
-// B bounds the sum of |terms| a slot can receive: every pair term obeys
-// |f(r) dr| <= 4.9 m / min(H_i, H_j)^2 and |phi| <= 3.9 m / min(H_i, H_j)
-// (the largest values of the three softening kernels; Newtonian pairs
-// beyond max(H_i, H_j) obey m / H_j^2 and m / H_j), so with SYM_BOUND = 8
-//   B_acc = 8 M (1/H_j^2 + 1/H_min^2),   B_pot = 8 M (1/H_j + 1/H_min),
-// M and H_min being the set's total mass and smallest H (per row tile for
-// the local scale).  The error scale G^2 of the mirrored FP32 partials takes
-// the scale 2^(2e - SYM_LOCAL_BITS) locally and 2^(2E - SYM_G2_SHIFT) globally.
-constexpr int SYM_LOCAL_BITS = 62;
-constexpr int SYM_GLOBAL_BITS = 101;
-constexpr int SYM_LO_BITS = 40;
-constexpr int SYM_G2_SHIFT = 140;
-constexpr float SYM_BOUND = 8.f;
-constexpr int SYM_E_NONE = -32768;     // slot takes no mirrored terms (padding, or no bound)
-constexpr int SYM_E_MAX = 120;          // local exponents are clamped to [-SYM_E_MAX, SYM_E_MAX]
-constexpr int SYM_E_GLOBAL_MAX = SYM_E_MAX + SYM_LO_BITS;
-
-// Slot word: int16 acc exponent in the low half, int16 pot exponent in the high half.
-__host__ __device__ inline int sym_word(int ea, int ep)
-{
-    return (int)(((unsigned)ep << 16) | ((unsigned)ea & 0xffffu));
-}
-__host__ __device__ inline int sym_exp_acc(int w) { return (int)(short)(w & 0xffff); }
-__host__ __device__ inline int sym_exp_pot(int w) { return (int)(short)((unsigned)w >> 16); }
-
-// Local exponent for a bound B computed in FP32: B < 2^x with x from the
-// float's exponent field (denormals and zero: 2^-126); clamped to
-// [-SYM_E_MAX, SYM_E_MAX]; `fallback` when B is not finite.
-__device__ __forceinline__ int sym_local_exp(float B, int fallback)
-{
-    const int bits = __float_as_int(B);
-    const int ef = (bits >> 23) & 0xff;
-    if (ef == 0xff) return fallback;                // inf or NaN
-    const int x = ef == 0 ? -126 : ef - 126;
-    return min(max(SYM_LOCAL_BITS - x, -SYM_E_MAX), SYM_E_MAX);
-}
-__device__ __forceinline__ float exp2f_int(int e)  // 2^e, |e| <= 126
-{
-    return __int_as_float((e + 127) << 23);
-}
-__device__ __forceinline__ double exp2d_int(int e)  // 2^e, |e| <= 1022
-{
-    return __longlong_as_double((long long)(e + 1023) << 52);
-}
-
-// q * 2^s as hi * 2^SYM_LO_BITS + lo with 0 <= lo < 2^SYM_LO_BITS (s <= SYM_LO_BITS;
-// s < 0 rounds half up).  |q| <= 2^62.
-__host__ __device__ inline void sym_split(long long q, int s, long long &hi, long long &lo)
-{
-    if (s >= 0) {
-        const int r = SYM_LO_BITS - s;
-        hi = q >> r;
-        lo = (q - (hi << r)) << s;
-    } else {
-        const long long v = s <= -63 ? 0ll : (q + (1ll << (-s - 1))) >> (-s);
-        hi = v >> SYM_LO_BITS;
-        lo = v - (hi << SYM_LO_BITS);
-    }
-}
-// q * 2^s in one word (s <= 2; the caller's bound keeps the result in range).
-__host__ __device__ inline long long sym_shift(long long q, int s)
-{
-    if (s >= 0) return q << s;
-    if (s <= -63) return 0ll;
-    return (q + (1ll << (-s - 1))) >> (-s);
 }
 
 // ------------------------------------------ bulk async copies (TMA, 1-D)

@@ -46,10 +46,6 @@ cudaError_t launch_itile_meta(const SetDesc *sets, int nsets, int ntiles_total,
                               const SortedF64 D, ITileMeta *meta, cudaStream_t st);
 cudaError_t launch_jmeta(const SetDesc *sets, int nsets, int nmeta_total, const int *meta_set,
                          const SortedF64 D, JMeta *meta, cudaStream_t st);
-// Mutual-update kernel: per-set mass and smallest H^2 (stats, 2 per set) and
-// the per-slot exponent words of the mirrored terms' fixed-point sums.
-cudaError_t launch_sym_words(const SetDesc *sets, int nsets, int max_npad, const SortedF64 D,
-                             double *stats, int *words, cudaStream_t st);
 
 // --- compute kernels (sg_f64.cu, sg_f32.cu)
 struct ComputeArgs {
@@ -77,11 +73,6 @@ struct ComputeArgs {
     // split-FP32 built with -DSG_PHASES: [PHASE_COUNTERS] clock64 cycles per
     // phase summed over warps (see the Phase enum); nullptr = not counted
     unsigned long long *phases = nullptr;
-    // mutual-update kernel: integer sums of the mirrored terms ([9][jstride],
-    // zeroed before the launch) and the per-slot exponent words
-    long long *jacc = nullptr;
-    const int *jword = nullptr;
-    size_t jstride = 0;
 };
 
 // Phase accounting of the split-FP32 kernel (a diagnostic build: the pair
@@ -114,7 +105,6 @@ struct VariantInfo {
     int newton;     // one Newton step on rsqrt (f32 only)
     const char *name;
     int rows;       // rows per i-tile
-    int sym = 0;    // f32: mutual updates (whole sets only)
     int itile() const { return rows; }
 };
 int variant_count(int precision);
@@ -122,14 +112,6 @@ const VariantInfo &variant_info(int precision, int v);
 // Resident blocks per SM of variant v (queried once per process).
 int variant_occupancy(int precision, int v);
 cudaError_t launch_compute(int precision, int v, int grid, const ComputeArgs &a, cudaStream_t st);
-// mutual-update split-FP32 kernels (sg_f32sym.cu), listed after the one-sided
-// split-FP32 variants
-int sym_variant_count();
-const VariantInfo &sym_variant_info(int v);
-const void *sym_kernel(int v);
-int sym_smem_bytes(int v);
-cudaError_t sym_prepare(int v);
-cudaError_t launch_sym(int v, int grid, const ComputeArgs &a, cudaStream_t st);
 
 // --- merge and diagnostics (sg_prep.cu)
 // Refine test of the merge (split-FP32 calls): rows whose error scale G^2
@@ -140,11 +122,6 @@ struct MergeRefine {
     int *rcount = nullptr;         // [nsets] rows listed per set (zeroed before the merge)
     int *rlist = nullptr;          // listed sorted slots; set s at [S.ioff, S.ioff + S.ni)
     double *scale = nullptr;       // optional: G per row in the caller's order
-    // mutual-update kernel: the mirrored terms' integer sums ([9][jstride]:
-    // hi, lo of a_x, a_y, a_z, pot, then G^2) and the slot words (null: none)
-    const long long *jacc = nullptr;
-    const int *jword = nullptr;
-    size_t jstride = 0;
 };
 // tile_slots[t] = (first partial slot, j-chunk count) of global i-tile t.
 cudaError_t launch_merge(const SetDesc *sets, const int *tile_set, const int2 *tile_slots,

@@ -316,7 +316,6 @@ __global__ void k_itile_meta(const SetDesc *sets, const int *tile_set, int itile
     const int r0 = lt * itile;
     const int r1 = min(S.ni, r0 + itile);
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    double mass = 0.0, h2min = INFINITY;
     for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
         const int slot = ilist[S.ioff + r];
         const double v[3] = {D.x[slot], D.y[slot], D.z[slot]};
@@ -325,10 +324,8 @@ __global__ void k_itile_meta(const SetDesc *sets, const int *tile_set, int itile
             lo[d] = fmin(lo[d], v[d]);
             hi[d] = fmax(hi[d], v[d]);
         }
-        mass += D.m[slot];
-        h2min = fmin(h2min, D.h2[slot]);
     }
-    __shared__ double s_lo[3][32], s_hi[3][32], s_mass[32], s_h2[32];
+    __shared__ double s_lo[3][32], s_hi[3][32];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         for (int o = 16; o > 0; o >>= 1) {
@@ -339,15 +336,6 @@ __global__ void k_itile_meta(const SetDesc *sets, const int *tile_set, int itile
             s_lo[d][threadIdx.x >> 5] = lo[d];
             s_hi[d][threadIdx.x >> 5] = hi[d];
         }
-    }
-    // fixed reduction order: the mutual-update scales derive from these
-    for (int o = 16; o > 0; o >>= 1) {
-        mass += __shfl_xor_sync(0xffffffffu, mass, o);
-        h2min = fmin(h2min, __shfl_xor_sync(0xffffffffu, h2min, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        s_mass[threadIdx.x >> 5] = mass;
-        s_h2[threadIdx.x >> 5] = h2min;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -361,11 +349,6 @@ __global__ void k_itile_meta(const SetDesc *sets, const int *tile_set, int itile
             }
             c[d] = l <= h ? 0.5 * (l + h) : 0.0;
         }
-        double ms = s_mass[0], hm = s_h2[0];
-        for (int w = 1; w < nw; w++) {
-            ms += s_mass[w];
-            hm = fmin(hm, s_h2[w]);
-        }
         ITileMeta M;
         M.chx = __double2float_rn(c[0]);
         M.chy = __double2float_rn(c[1]);
@@ -373,9 +356,7 @@ __global__ void k_itile_meta(const SetDesc *sets, const int *tile_set, int itile
         M.clx = __double2float_rn(c[0] - (double)M.chx);
         M.cly = __double2float_rn(c[1] - (double)M.chy);
         M.clz = __double2float_rn(c[2] - (double)M.chz);
-        // bounds: mass rounded up, H^2 down
-        M.mass = __double2float_ru(ms);
-        M.h2min = hm < INFINITY ? __double2float_rd(hm) : 0.f;
+        M.pad_[0] = M.pad_[1] = 0.f;
         meta[t] = M;
     }
 }
@@ -387,84 +368,6 @@ cudaError_t launch_itile_meta(const SetDesc *sets, int nsets, int ntiles_total,
     (void)nsets;
     if (ntiles_total <= 0) return cudaSuccess;
     k_itile_meta<<<ntiles_total, 128, 0, st>>>(sets, tile_set, itile, ilist, D, meta);
-    ++g_launches;
-    return cudaGetLastError();
-}
-
-// ------------------------------------------- mutual-update scales (global)
-// Per set: total mass and smallest H^2, in a fixed reduction order (the
-// per-slot exponents derive from them, so they must not vary between calls).
-__global__ void k_sym_setstats(const SetDesc *sets, SortedF64 D, double *stats)
-{
-    const SetDesc S = sets[blockIdx.x];
-    double mass = 0.0, h2min = INFINITY;
-    for (int k = threadIdx.x; k < S.n; k += blockDim.x) {
-        mass += D.m[S.poff + k];
-        h2min = fmin(h2min, D.h2[S.poff + k]);
-    }
-    __shared__ double s_m[32], s_h[32];
-    for (int o = 16; o > 0; o >>= 1) {
-        mass += __shfl_xor_sync(0xffffffffu, mass, o);
-        h2min = fmin(h2min, __shfl_xor_sync(0xffffffffu, h2min, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        s_m[threadIdx.x >> 5] = mass;
-        s_h[threadIdx.x >> 5] = h2min;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double ms = s_m[0], hm = s_h[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
-            ms += s_m[w];
-            hm = fmin(hm, s_h[w]);
-        }
-        stats[2 * blockIdx.x] = ms;
-        stats[2 * blockIdx.x + 1] = hm;
-    }
-}
-
-// Bound of a positive finite double: B < 2^x (denormals: x = -1022).
-__device__ __forceinline__ int dbl_log2_bound(double B)
-{
-    const int eb = (int)((__double_as_longlong(B) >> 52) & 0x7ff);
-    return eb == 0 ? -1022 : eb - 1022;
-}
-
-// Per sorted slot the word of global exponents (sym_word), SYM_E_NONE for
-// padding and for slots whose bound is not finite or too large for the
-// local scales (their rows go to the FP64 refine).
-__global__ void k_sym_words(const SetDesc *sets, SortedF64 D, const double *stats, int *words)
-{
-    const SetDesc S = sets[blockIdx.y];
-    const double M = stats[2 * blockIdx.y], hm = stats[2 * blockIdx.y + 1];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S.npad; k += gridDim.x * blockDim.x) {
-        int w = sym_word(SYM_E_NONE, SYM_E_NONE);
-        if (k < S.n) {
-            const double h2 = D.h2[S.poff + k];
-            const double Ba = (double)SYM_BOUND * M * (1.0 / h2 + 1.0 / hm);
-            const double Bp = (double)SYM_BOUND * M * (1.0 / sqrt(h2) + 1.0 / sqrt(hm));
-            if (Ba > 0.0 && Ba < INFINITY && Bp > 0.0 && Bp < INFINITY) {
-                const int xa = dbl_log2_bound(Ba), xp = dbl_log2_bound(Bp);
-                // x <= 180 keeps every local exponent within the float scales
-                if (xa <= 180 && xp <= 180)
-                    w = sym_word(min(SYM_GLOBAL_BITS - xa, SYM_E_GLOBAL_MAX),
-                                 min(SYM_GLOBAL_BITS - xp, SYM_E_GLOBAL_MAX));
-            }
-        }
-        words[S.poff + k] = w;
-    }
-}
-
-cudaError_t launch_sym_words(const SetDesc *sets, int nsets, int max_npad, const SortedF64 D,
-                             double *stats, int *words, cudaStream_t st)
-{
-    if (nsets <= 0) return cudaSuccess;
-    k_sym_setstats<<<nsets, 1024, 0, st>>>(sets, D, stats);
-    ++g_launches;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    dim3 grid(grid_for(max_npad, 256, 1024), nsets);
-    k_sym_words<<<grid, 256, 0, st>>>(sets, D, stats, words);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -580,23 +483,6 @@ __global__ void k_merge(const SetDesc *sets, const int *tile_set, const int2 *ti
             if (R.gpart) g2 += R.gpart[slot * itile + li];
         }
         const int slot = ilist[S.ioff + r0 + li];
-        if (R.jacc) {
-            // mirrored terms of the mutual-update kernel (stored negated)
-            const int w = R.jword[slot];
-            const int ea = sym_exp_acc(w), ep = sym_exp_pot(w);
-            if (ea == SYM_E_NONE || ep == SYM_E_NONE) {
-                g2 = INFINITY;  // no bound: the FP64 refine recomputes the row
-            } else {
-                const size_t js = R.jstride;
-                for (int q = 0; q < 4; q++) {
-                    const int e = q < 3 ? ea : ep;
-                    const double v = (double)R.jacc[(2 * q) * js + slot] * exp2d_int(SYM_LO_BITS - e) +
-                                     (double)R.jacc[(2 * q + 1) * js + slot] * exp2d_int(-e);
-                    acc[q] -= v;
-                }
-                g2 += (float)((double)R.jacc[8 * js + slot] * exp2d_int(SYM_G2_SHIFT - 2 * ea));
-            }
-        }
         const int o = D.orig[slot];
         out.ax[o] = acc[0];
         out.ay[o] = acc[1];
