@@ -134,6 +134,7 @@ struct Plan {
     std::vector<int> offsets;
     bool full_rows = true;
     int i_lo = 0, ni = 0, precision = -1, variant = -1;
+    bool tree = false;  // Barnes-Hut call: the octree's levels are the full curve key
     // derived
     int nsets = 0, ntot = 0, npad_tot = 0, rows_tot = 0, ntiles = 0, nmeta = 0, nitems = 0;
     int nslots = 0, itile = 0, tj = 0, max_n = 0, max_npad = 0, bits = 21, end_bit = 63;
@@ -381,7 +382,7 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
 // of the variant on the device), so it also runs without a GPU
 // (sphgrav_plan_preview).
 static int build_plan(int resident, const std::vector<int> &offsets, bool full_rows, int i_lo,
-                      int ni, int precision, int variant, Plan &P)
+                      int ni, int precision, int variant, Plan &P, bool tree = false)
 {
     const VariantInfo &V = variant_info(precision, variant);
     P = Plan();
@@ -391,6 +392,7 @@ static int build_plan(int resident, const std::vector<int> &offsets, bool full_r
     P.ni = ni;
     P.precision = precision;
     P.variant = variant;
+    P.tree = tree;
     P.nsets = (int)offsets.size() - 1;
     P.itile = V.itile();
     P.tj = V.tj;
@@ -522,31 +524,37 @@ static int build_plan(int resident, const std::vector<int> &offsets, bool full_r
     P.nslots = slot;
     P.grid = std::max(1, std::min(P.nitems, resident));
     const int setbits = ceil_log2(std::max(1, P.nsets));
-    P.bits = std::min(21, (64 - setbits) / 3);
+    // Curve-key bits per axis.  The octree's levels are the key's 3-bit
+    // digits, so tree calls keep 21; the direct sums only need cells fine
+    // enough that particles rarely share one (2^(3b) cells, about 2^15 per
+    // particle of the largest set, at least 2^10 per axis), and every 8 key
+    // bits cost the sort a pass (16K: 4 passes instead of 8).
+    const int want = tree ? 21 : std::max(10, (ceil_log2(std::max(2, P.max_n)) + 2) / 3 + 5);
+    P.bits = std::min(std::min(21, want), (64 - setbits) / 3);
     P.end_bit = 3 * P.bits + setbits;
     P.valid = true;
     return SPHGRAV_OK;
 }
 
 static bool plan_matches(const Plan &P, const std::vector<int> &offsets, bool full_rows, int i_lo,
-                         int ni, int precision, int variant)
+                         int ni, int precision, int variant, bool tree)
 {
     return P.valid && P.offsets == offsets && P.full_rows == full_rows &&
            (full_rows || (P.i_lo == i_lo && P.ni == ni)) && P.precision == precision &&
-           P.variant == variant;
+           P.variant == variant && P.tree == tree;
 }
 
 static int prepare(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
-                   int ni, int precision, int variant)
+                   int ni, int precision, int variant, bool tree = false)
 {
-    if (!plan_matches(c->plan, offsets, full_rows, i_lo, ni, precision, variant)) {
+    if (!plan_matches(c->plan, offsets, full_rows, i_lo, ni, precision, variant, tree)) {
         if (c->capturing)
             return set_err(SPHGRAV_ERR_PROTOCOL,
                            "work plan changed during a graph capture; call the entry point once "
                            "with the same sizes before capturing");
         Plan P;
         TRY(build_plan(variant_occupancy(precision, variant) * c->sm_count, offsets, full_rows,
-                       i_lo, ni, precision, variant, P));
+                       i_lo, ni, precision, variant, P, tree));
         ++c->epoch;  // graphs captured under the old plan must not replay
         TRY(ensure(c, c->sets, std::max(1, P.nsets), "sets"));
         TRY(ensure(c, c->tile_set, std::max(1, P.ntiles), "tile_set"));
@@ -656,7 +664,7 @@ static SortedF32 sorted32(sphgrav_ctx *c)
 static int run_tree(sphgrav_ctx *c, const std::vector<int> &offsets, bool full_rows, int i_lo,
                     int ni, const InputsDev &in, const OutputsDev &out, double *W, int nkernel)
 {
-    TRY(prepare(c, offsets, full_rows, i_lo, ni, SPHGRAV_FP64, 0));
+    TRY(prepare(c, offsets, full_rows, i_lo, ni, SPHGRAV_FP64, 0, true));
     const Plan &P = c->plan;
     cudaStream_t st = c->stream;
     const int n = P.ntot, nslots = P.npad_tot, nsets = P.nsets;
