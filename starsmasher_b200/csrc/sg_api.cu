@@ -525,11 +525,17 @@ static int build_plan(int resident, const std::vector<int> &offsets, bool full_r
     P.grid = std::max(1, std::min(P.nitems, resident));
     const int setbits = ceil_log2(std::max(1, P.nsets));
     // Curve-key bits per axis.  The octree's levels are the key's 3-bit
-    // digits, so tree calls keep 21; the direct sums only need cells fine
-    // enough that particles rarely share one (2^(3b) cells, about 2^15 per
-    // particle of the largest set, at least 2^10 per axis), and every 8 key
-    // bits cost the sort a pass (16K: 4 passes instead of 8).
-    const int want = tree ? 21 : std::max(10, (ceil_log2(std::max(2, P.max_n)) + 2) / 3 + 5);
+    // digits, so tree calls keep 21.  For the direct sums every 8 key bits
+    // cost the sort a pass, which matters only for small sets: up to 65,536
+    // particles they take cells just fine enough that particles rarely
+    // share one (2^(3b) cells, about 2^15 per particle, at least 2^10 per
+    // axis; 16K: 4 passes instead of 8).  Larger sets keep 21 bits: a curve
+    // of another order has another orientation, so it tiles a centred star
+    // differently (on the 1M red giant 18 refined rows instead of 8, RMS
+    // error 6.2e-8 instead of 4.7e-8), for a sort that is < 0.1% of the call.
+    const int want = (tree || P.max_n > 65536)
+                         ? 21
+                         : std::max(10, (ceil_log2(std::max(2, P.max_n)) + 2) / 3 + 5);
     P.bits = std::min(std::min(21, want), (64 - setbits) / 3);
     P.end_bit = 3 * P.bits + setbits;
     P.valid = true;
