@@ -290,6 +290,10 @@ static int use_device(sphgrav_ctx *c)
 
 // ------------------------------------------------------- variant choice
 static const int kMinChunkJ = 2048;  // shortest j-chunk worth a partial slot
+// The FP64 kernel's items are slower per source, so a short chunk still
+// outweighs its partial slot; small sets need them to fill the GPU (16K:
+// 1,024 items of 2,048 sources left a third of the SMs idle at the end).
+static const int kMinChunkJ64 = 512;
 // FP64 variant that recomputes the refine-listed rows (few rows per set: the
 // smallest row tile)
 static const int kRefineVariant = 0;
@@ -339,14 +343,13 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
     }
     const bool batch = offsets.size() > 2;
     // FP64 (kernel ms on B200): one-warp CTAs with two rows per thread and
-    // 128-source tiles from 2^16 on, and for batches from 2^15 (64K: 6.40 vs
-    // 6.94 for one row per thread; 131K: 22.2 vs 24.0; 262K: 83.8 vs 86.7 for
-    // two rows in 4-warp CTAs; 1M: 1253 vs 1253; the batch of 4K-131K models:
-    // 157 vs 170; the 16 collision snapshots: 1397 vs 1450), one row per
-    // thread and 128-source tiles below (8K: 0.74 vs 1.11; 16K: 1.04 vs 1.32;
-    // 32K: 2.33 vs 2.42).  One-warp CTAs wait only on their own warp at the
-    // per-tile stage release.
-    if (precision == SPHGRAV_FP64) return (b >= 16 || (batch && b >= 15)) ? 9 : 0;
+    // 128-source tiles from 2^15 on (32K: 2.16 vs 2.23 for one row per thread;
+    // 64K: 6.32 vs 6.66; 131K: 22.2 vs 24.0; 262K: 83.8 vs 86.7 for two rows
+    // in 4-warp CTAs; 1M: 1253 vs 1253; the batch of 4K-131K models: 157 vs
+    // 170; the 16 collision snapshots: 1397 vs 1450), one row per thread and
+    // 128-source tiles below (16K: 0.80 vs 0.90).  One-warp CTAs wait only on
+    // their own warp at the per-tile stage release.
+    if (precision == SPHGRAV_FP64) return b >= 15 ? 9 : 0;
     // split-FP32 defaults by pair-weighted mean N = 2^b, from sweeps on B200
     // (pair-kernel ms of the chosen shape vs the runner-up):
     //   b >= 20, and batches from 2^18: W12K2Q1, 7 stages (1M: 488.5; the
@@ -425,13 +428,14 @@ static int build_plan(int resident, const std::vector<int> &offsets, bool full_r
     P.ntiles = (int)toff;
     P.nmeta = (int)moff;
     const int target = 4 * resident;
+    const int min_chunk = precision == SPHGRAV_FP64 ? kMinChunkJ64 : kMinChunkJ;
     // One set: items are all alike, so pick the chunk count whose item count
     // fills the last wave of persistent CTAs best (ties: fewer chunks).
     int single_nch = 0;
     if (P.nsets == 1 && P.ntiles > 0) {
         const SetDesc &d = P.sets[0];
         const int jtiles = (d.n + P.tj - 1) / P.tj;
-        const int maxch = std::max(1, std::min(jtiles, std::min(64, (int)(((long long)jtiles * P.tj) / kMinChunkJ))));
+        const int maxch = std::max(1, std::min(jtiles, std::min(64, (int)(((long long)jtiles * P.tj) / min_chunk))));
         // item costs differ (near-field work is uneven), so small sets want
         // several items per CTA for the queue to balance them
         const int nch_min = std::min(maxch, std::max(1, (3 * resident + P.ntiles - 1) / P.ntiles));
@@ -457,7 +461,7 @@ static int build_plan(int resident, const std::vector<int> &offsets, bool full_r
     std::vector<int> tile_nch(P.ntiles, 1);
     auto set_maxch = [&](const SetDesc &d) {
         const int jtiles = (d.n + P.tj - 1) / P.tj;
-        return std::max(1, std::min(jtiles, (int)(((long long)jtiles * P.tj) / kMinChunkJ)));
+        return std::max(1, std::min(jtiles, (int)(((long long)jtiles * P.tj) / min_chunk)));
     };
     if (P.ntiles <= 2 * resident || precision != SPHGRAV_F32SPLIT) {
         for (int s = 0; s < P.nsets; s++) {
