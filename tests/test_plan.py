@@ -86,3 +86,18 @@ def test_preview_rejects_bad_arguments():
                             ([0, 5], "f32split", 99)):
         with pytest.raises(_lib.SphgravError):
             api.plan_preview(offs, prec, var)
+
+
+def test_fp64_small_set_fills_the_gpu():
+    """The FP64 kernel's small sets take chunks down to 512 sources, so a
+    16K set gives each of 592 persistent CTAs several items (with the
+    split-FP32 minimum of 2,048 sources it had 1,024 items, under two per
+    CTA, and a third of the SMs idle at the end)."""
+    resident = 148 * 4
+    p, by_tile = _check_plan([0, 16384], "fp64", 0, resident)
+    assert p["nitems"] >= 4 * resident
+    for chunks in by_tile.values():
+        assert all(je - jb >= 512 for _, _, jb, je in chunks)
+    # split-FP32 keeps its 2,048-source minimum
+    p32, by32 = _check_plan([0, 16384], "f32split", 5, 148)
+    assert all(je - jb >= 2048 for ch in by32.values() for _, _, jb, je in ch)
