@@ -342,14 +342,21 @@ static int choose_variant(sphgrav_ctx *c, int precision, const std::vector<int> 
         if (v >= 0) return v;
     }
     const bool batch = offsets.size() > 2;
-    // FP64 (kernel ms on B200): one-warp CTAs with two rows per thread and
-    // 128-source tiles from 2^15 on (32K: 2.16 vs 2.23 for one row per thread;
-    // 64K: 6.32 vs 6.66; 131K: 22.2 vs 24.0; 262K: 83.8 vs 86.7 for two rows
-    // in 4-warp CTAs; 1M: 1253 vs 1253; the batch of 4K-131K models: 157 vs
-    // 170; the 16 collision snapshots: 1397 vs 1450), one row per thread and
-    // 128-source tiles below (16K: 0.80 vs 0.90).  One-warp CTAs wait only on
-    // their own warp at the per-tile stage release.
-    if (precision == SPHGRAV_FP64) return b >= 15 ? 9 : 0;
+    // FP64 (kernel ms on B200), 128-source tiles throughout.  One-warp CTAs
+    // wait only on their own warp at the per-tile stage release.
+    //   single sets 2^13..2^16: one-warp CTAs, one row per thread (16K: 0.80
+    //     vs 0.81 for 4-warp CTAs; 32K: 1.93 vs 2.18 for two rows per
+    //     thread; 64K: 6.13 vs 6.32)
+    //   from 2^17, and batches from 2^15: one-warp CTAs, two rows per thread
+    //     (131K: 21.9 vs 23.1 for one row; 262K: 81.9 vs 88.0; 1M: 1235 vs
+    //     1356; the batch of 4K-131K models: 156 vs 170; the 16 collision
+    //     snapshots: 1396 vs 1535)
+    //   below: 4-warp CTAs, one row per thread
+    if (precision == SPHGRAV_FP64) {
+        if (b >= 17 || (batch && b >= 15)) return 9;
+        if (!batch && b >= 13) return 13;
+        return 0;
+    }
     // split-FP32 defaults by pair-weighted mean N = 2^b, from sweeps on B200
     // (pair-kernel ms of the chosen shape vs the runner-up):
     //   b >= 20, and batches from 2^18: W12K2Q1, 7 stages (1M: 488.5; the

@@ -291,7 +291,9 @@ __global__ void __launch_bounds__(NT, F64Occ<NT, K, MB>::MINB) k_fp64(ComputeArg
     X(32, 2, 128, 3, 2, 0, "fp64_nt32_k2_tj128")             \
     X(128, 2, 256, 3, 1, 4, "fp64_nt128_k2_tj256_u1_b4")     \
     X(64, 3, 256, 3, 2, 0, "fp64_nt64_k3_tj256")             \
-    X(128, 1, 64, 3, 2, 0, "fp64_nt128_k1_tj64")
+    X(128, 1, 64, 3, 2, 0, "fp64_nt128_k1_tj64")            \
+    X(32, 1, 128, 3, 2, 0, "fp64_nt32_k1_tj128")             \
+    X(64, 1, 128, 3, 2, 0, "fp64_nt64_k1_tj128")
 
 #define SG_INFO(NT, K, TJ, NS, U, MB, NAME) {0, NT, K, 1, TJ, 0, NAME, NT * K},
 static const VariantInfo kF64Variants[] = {SG_F64_VARIANTS(SG_INFO)};
